@@ -1,0 +1,210 @@
+/*
+ * tsne_h2pack.h -- C ABI of the B200 t-SNE optimisation engine.
+ *
+ * Drop-in for the reference's C ABI (include/tsne_h2pack.h of xinxing02/tsne-h2pack-python):
+ * the same types, layouts and entry points, bound by the reference's own Python loader
+ * (tsne_h2pack/_backend.py:345-448). Every entry point below names the reference
+ * declaration it replaces. Plain C types only; all device state stays behind the opaque
+ * workspace.
+ *
+ * Differences a caller can observe:
+ *   - tsne_workspace_t is opaque (the reference's Python treats it as opaque too,
+ *     _backend.py:123-127); H2Pack_p is an opaque handle to this engine's H2 matrix.
+ *   - num_threads only sets the host threads of compute_P_from_knn_distances' host
+ *     side; the optimisation runs on the current CUDA device.
+ *   - Diagnostics go to stdout/stderr as in the reference; errors are reported through
+ *     the same NULL / non-zero returns.
+ */
+#ifndef TSNE_H2PACK_B200_H
+#define TSNE_H2PACK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* exported entry points (the library is built with hidden default visibility) */
+#ifndef TSNE_API
+#define TSNE_API __attribute__((visibility("default")))
+#endif
+
+#ifndef DTYPE
+#define DTYPE double
+#endif
+
+/* CSR matrix, int32 indices, double values (reference include/tsne_h2pack.h:17-24) */
+typedef struct {
+    int n_rows;
+    int n_cols;
+    int nnz;
+    int *row_ptr;
+    int *col_idx;
+    DTYPE *values;
+} sparse_matrix_t;
+
+/* Run parameters, 160 bytes, field for field the reference's layout
+ * (reference include/tsne_h2pack.h:27-85; mirrored by _backend.py:51-96). */
+typedef struct {
+    int n_iter;
+    DTYPE perplexity;
+    DTYPE learning_rate;          /* < 0: max(N / 12, 200) */
+    DTYPE momentum;
+    DTYPE initial_momentum;
+    int momentum_switch_iter;
+    DTYPE early_exag;
+    int early_exag_iter;
+    int use_vptree;               /* legacy k-NN selector of tsne_init; ignored */
+    DTYPE h2_tol;
+    int h2_rebuild_freq;
+    int h2pack_print_level;
+    int init_method;              /* 0: random N(0, 1e-4^2); 1: copy init_Y */
+    int random_seed;
+    int verbose;
+    int print_freq;
+    int enable_early_stopping;
+    DTYPE convergence_tol;
+    int convergence_patience;
+    int min_iter;
+    int sklearn_compatible;
+    int enable_profiling;
+    char *profiling_output_file;
+    int num_threads;
+    int h2_leaf_size;
+    int h2_rebuild_freq_early;
+    const DTYPE *init_Y;          /* low_dim x n_point, read only inside tsne_init* */
+} tsne_params_t;
+
+/* Per-iteration stage times in seconds (reference include/tsne_h2pack.h:88-99) */
+typedef struct {
+    double *knn_time;
+    double *p_construction_time;
+    double *p_matvec_time;
+    double *h2_rebuild_time;
+    double *h2_matvec_s_time;
+    double *h2_matvec_v_time;
+    double *z_computation_time;
+    double *gradient_time;
+    double *other_time;
+} profiling_data_t;
+
+typedef struct tsne_workspace tsne_workspace_t;      /* opaque */
+typedef struct tsne_h2_matrix *H2Pack_p;             /* opaque H2 matrix handle */
+
+/* ---- public API (reference include/tsne_h2pack.h:163-263) ---- */
+
+/* reference tsne_h2pack.h:167 / src/tsne_h2pack.c:56-104 */
+TSNE_API tsne_params_t tsne_create_default_params(void);
+
+/* reference tsne_h2pack.h:178; builds P from X with a brute-force k-NN (k = 3 * perplexity)
+ * on the device, then behaves like tsne_init_with_P */
+TSNE_API tsne_workspace_t *tsne_init(const DTYPE *X, int n_point, int pt_dim, int low_dim,
+                            const tsne_params_t *params);
+
+/* reference tsne_h2pack.h:196 / src/tsne_h2pack.c:1356-1547. Takes ownership of P (which
+ * must come from sparse_matrix_create); uploads P and the initial embedding and builds
+ * the first H2 matrix on the device. NULL on bad low_dim or P shape, or a failed build. */
+TSNE_API tsne_workspace_t *tsne_init_with_P(const DTYPE *X, int n_point, int pt_dim, int low_dim,
+                                   const tsne_params_t *params, sparse_matrix_t *P);
+
+/* reference tsne_h2pack.h:210 / src/tsne_h2pack.c:1652-2102. 0 on success, -1 on a failed
+ * H2 rebuild (e.g. non-finite coordinates) or a device error. */
+TSNE_API int tsne_run(tsne_workspace_t *workspace);
+
+/* reference tsne_h2pack.h:217 / src/tsne_h2pack.c:2108-2122: low_dim x n_point, caller's order */
+TSNE_API void tsne_get_embedding(tsne_workspace_t *workspace, DTYPE *Y_out);
+
+/* reference tsne_h2pack.h:223 / src/tsne_h2pack.c:2128-2184 */
+TSNE_API void tsne_destroy(tsne_workspace_t *workspace);
+
+/* reference tsne_h2pack.h:236 / src/tsne_h2pack.c:2190-2212 */
+TSNE_API int tsne_fit_transform(const DTYPE *X, int n_point, int pt_dim, int low_dim,
+                       const tsne_params_t *params, DTYPE *Y_out);
+
+/* reference tsne_h2pack.h:256 / src/tsne_h2pack.c:2214-2236 */
+TSNE_API int tsne_fit_transform_with_P(const DTYPE *X, int n_point, int pt_dim, int low_dim,
+                              const tsne_params_t *params, sparse_matrix_t *P, DTYPE *Y_out);
+
+/* ---- sparse matrix utilities (reference tsne_h2pack.h:269-295, src/tsne_utils.c:18-60) ---- */
+TSNE_API sparse_matrix_t *sparse_matrix_create(int n_rows, int n_cols, int nnz);
+TSNE_API void sparse_matrix_destroy(sparse_matrix_t *mat);
+TSNE_API void sparse_matvec(const sparse_matrix_t *A, const DTYPE *x, DTYPE *y);
+
+/* ---- internal functions exposed for testing (reference tsne_h2pack.h:301-446) ---- */
+
+/* reference tsne_h2pack.h:312 / src/tsne_utils.c:828-933 (device brute-force k-NN here) */
+TSNE_API sparse_matrix_t *compute_sparse_P(const DTYPE *X, int n_point, int pt_dim, DTYPE perplexity,
+                                  int use_vptree, int verbose, int num_threads);
+
+/* reference tsne_h2pack.h:338 / src/tsne_utils.c:1022-1105: conditional P_j|i by FP64 beta
+ * bisection on the device; returns a C-allocated matrix (free with sparse_matrix_destroy) */
+TSNE_API sparse_matrix_t *compute_P_from_knn_distances(const DTYPE *knn_distances, const int *knn_indices,
+                                              const int *knn_indptr, int n_samples, int nnz,
+                                              DTYPE perplexity, int num_threads);
+
+/* reference tsne_h2pack.h:358 / src/tsne_utils.c:1111-1150 (host; the same generator) */
+TSNE_API void initialize_embedding(DTYPE *Y, int n_point, int low_dim, int method, const DTYPE *Y0,
+                          unsigned int seed);
+
+/* reference tsne_h2pack.h:377 / src/tsne_h2pack.c:290-356: grad += attractive force,
+ * host arrays in, host array out (computed on the device) */
+TSNE_API void compute_attractive_forces(const sparse_matrix_t *P, const DTYPE *Y, int low_dim, int n_point,
+                               DTYPE early_exag, DTYPE *grad, int num_threads);
+
+/* reference tsne_h2pack.h:398 / src/tsne_h2pack.c:389-630: grad -= repulsive force of the
+ * workspace's current H2 matrix (exact O(N^2) sums when h2pack_W is NULL); returns Z */
+TSNE_API DTYPE compute_repulsive_forces_h2pack(H2Pack_p h2pack_W, const DTYPE *Y, int low_dim, int n_point,
+                                      tsne_workspace_t *workspace, DTYPE *grad, int iter);
+
+/* reference tsne_h2pack.h:413 / src/tsne_h2pack.c:772-953: rebuild the workspace's H2 matrix
+ * for its current embedding; 0 on success, -1 on failure */
+TSNE_API int update_h2_matrix(tsne_workspace_t *workspace, int force_rebuild);
+
+/* reference tsne_h2pack.h:420 / src/tsne_h2pack.c:2243-2247: last KL divergence */
+TSNE_API DTYPE compute_kl_divergence(tsne_workspace_t *workspace);
+
+/* reference tsne_h2pack.h:427 / src/tsne_h2pack.c:1553-1628: same CSV schema */
+TSNE_API void tsne_write_profiling_data(tsne_workspace_t *workspace, const char *filename);
+
+/* reference tsne_h2pack.h:436 / src/tsne_h2pack.c:1634-1646 */
+TSNE_API void tsne_set_init_profiling_times(tsne_workspace_t *workspace, double knn_time,
+                                   double p_construction_time);
+
+/* reference tsne_h2pack.h:441 / src/tsne_h2_matmul.c:225-452: Y[c] = W X[c] for nv columns
+ * (host arrays of length n, the caller's order). Returns -1 if unsupported. */
+TSNE_API int tsne_h2_matmul(H2Pack_p h2, const int nv, const DTYPE *const *X, DTYPE *const *Y, void **ws);
+TSNE_API void tsne_h2_matmul_free(void **ws);
+
+/* reference tsne_h2pack.h:446 / src/tsne_reorder.c:112-167: new point k = old point ord[k] */
+TSNE_API int tsne_renumber_points(tsne_workspace_t *workspace, const int *ord, int num_threads);
+
+/* ---- engine inspection (no reference counterpart: lets host tests compare the device
+ * H2 matrix with the oracle; all arrays are host arrays) ---- */
+
+/* The workspace's current H2 matrix, or NULL when the exact path is in use */
+TSNE_API H2Pack_p tsne_get_h2_matrix(tsne_workspace_t *workspace);
+/* n_node, max_level, total far entries, total near entries */
+TSNE_API int tsne_h2_info(H2Pack_p h2, int *n_node, int *max_level, int *n_far, int *n_near);
+/* tree position -> current point number (n), root corner (low_dim) and half-width */
+TSNE_API int tsne_h2_get_tree(H2Pack_p h2, int *perm, double *corner, double *radius);
+/* node table (n_node each): start, end, level, parent, first child, child count, leaf flag */
+TSNE_API int tsne_h2_get_nodes(H2Pack_p h2, int *start, int *end, int *level, int *parent,
+                      int *first_child, int *n_child, int *is_leaf);
+/* per-target CSR of far and near partners (n_node + 1 pointers; partners ascending) */
+TSNE_API int tsne_h2_get_lists(H2Pack_p h2, int *far_ptr, int *far_idx, int *near_ptr, int *near_idx);
+/* per-node skeleton rank (n_node) */
+TSNE_API int tsne_h2_get_ranks(H2Pack_p h2, int *rank);
+/* Current device state in the caller's order: Y (low_dim x n_point), and the repulsive
+ * force of the last rebuild (low_dim x n_point, NULL to skip) */
+TSNE_API int tsne_get_state(tsne_workspace_t *workspace, DTYPE *Y_out, DTYPE *rep_out, DTYPE *rep_Z);
+/* Replace the embedding (low_dim x n_point, caller's order) and reset gains / velocity */
+TSNE_API int tsne_set_embedding(tsne_workspace_t *workspace, const DTYPE *Y_in);
+/* Run iterations [iter_begin, iter_end) of the schedule (tsne_run = [0, n_iter)) */
+TSNE_API int tsne_run_range(tsne_workspace_t *workspace, int iter_begin, int iter_end);
+/* Number of H2 rebuilds and kernel launches issued by the last tsne_run / tsne_run_range */
+TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, long long *n_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

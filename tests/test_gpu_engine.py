@@ -1,0 +1,210 @@
+"""Parity of the device engine (through its C ABI) with the oracle and the reference.
+
+Tolerances (FP32 device state against FP64 oracles; t-SNE amplifies a rounding difference
+by roughly 2x per iteration, so trajectory comparisons stop after a few tens of
+iterations):
+  - exact path, 20 iterations, vs the reference's own build: max rel 2e-3
+  - perplexity calibration vs the oracle: rtol 1e-10
+  - H2 tree permutation, node table and near/far lists vs the oracle: bit-exact
+  - H2 repulsive force vs the FP64 exact force: rel 2-norm <= h2_tol
+  - attractive force vs the FP64 oracle: rel 1e-5
+  - 1000-iteration run: KL within 1% of the oracle's run, 30-NN preservation within 0.5 points
+"""
+import ctypes
+
+import numpy as np
+import pytest
+from scipy.sparse import csr_matrix
+
+import oracle as O
+from helpers import Engine, knn_preservation, problem, rel, rel2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    return problem(1000, seed=0)
+
+
+@pytest.fixture(scope="module")
+def mid():
+    return problem(5000, seed=1, n_clusters=12, dim=20)
+
+
+def test_exact_path_matches_reference(small):
+    """N < 2000 runs the exact O(N^2) repulsion every iteration, as the reference does."""
+    X, G, P, _ = small
+    Y0 = O.init_embedding(P.shape[0], 2, 11)
+    eng = Engine(P, Y0, n_iter=20, learning_rate=200.0)
+    eng.run_all()
+    Y = eng.embedding()
+    if O.ref_available():
+        Yr, klr = O.ref_run(P, Y0, 20, learning_rate=200.0)
+    else:
+        Yr, klr = O.run(P, Y0, n_iter=20, learning_rate=200.0, use_h2=False)
+    assert rel(Y, Yr) < 2e-3
+    assert abs(eng.kl() - klr) < 1e-3 * abs(klr)
+
+
+def test_exact_method_matches_oracle(mid):
+    """method='exact' (h2_rebuild_freq = 999999) at N >= 2000."""
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 2, 5)
+    eng = Engine(P, Y0, n_iter=15, exact=True)
+    eng.run_all()
+    Yo, klo = O.run(P, Y0, n_iter=15, use_h2=False)
+    assert rel(eng.embedding(), Yo) < 2e-3
+    assert abs(eng.kl() - klo) < 1e-3 * abs(klo)
+
+
+def test_conditional_P_matches_oracle(small):
+    from tsne_h2pack._backend import get_backend
+    X, G, P, _ = small
+    Pc = get_backend().conditional_P(G, 30.0)
+    ref = O.conditional_P(G.data, G.indptr, 30.0)
+    np.testing.assert_allclose(Pc.data, ref, rtol=1e-10, atol=1e-300)
+
+
+@pytest.mark.parametrize("scale", [1e-3, 1.0, 1e3, 1e6])
+def test_calibration_known_answers(scale):
+    """Rows sum to 1 and hit perplexity 30; scale invariant (the reference's
+    tests/test_perplexity_calibration.py:18-59 on the same fixture)."""
+    from tsne_h2pack._backend import get_backend
+    rng = np.random.default_rng(0)
+    d = np.sort(rng.uniform(1.0, 3.0, size=(200, 90)), axis=1)
+    n, k = d.shape
+    G = csr_matrix((d.ravel() * scale, np.tile(np.arange(k), n), np.arange(0, (n + 1) * k, k)), shape=(n, 200))
+    be = get_backend()
+    Pc = be.conditional_P(G, 30.0).toarray()[:, :k]
+    base = be.conditional_P(csr_matrix((d.ravel(), G.indices, G.indptr), shape=(n, 200)), 30.0).toarray()[:, :k]
+    np.testing.assert_allclose(Pc.sum(axis=1), 1.0, rtol=1e-10)
+    H = -np.sum(np.where(Pc > 0, Pc * np.log2(np.maximum(Pc, 1e-300)), 0.0), axis=1)
+    np.testing.assert_allclose(2.0 ** H, 30.0, rtol=1e-3)
+    np.testing.assert_allclose(Pc, base, rtol=1e-3, atol=1e-9)
+
+
+def _evolved(P, n_iter, seed):
+    Y0 = O.init_embedding(P.shape[0], 2, seed)
+    Y, _ = O.run(P, Y0, n_iter=n_iter)
+    return Y
+
+
+@pytest.mark.parametrize("n_iter", [20, 300])
+def test_tree_and_lists_bit_exact(mid, n_iter):
+    X, G, P, _ = mid
+    Y = _evolved(P, n_iter, 2).astype(np.float32).astype(np.float64)
+    eng = Engine(P, Y, n_iter=1)
+    assert eng.rebuild() == 0
+    dev = eng.h2()
+    assert dev is not None
+    h = O.H2(Y, leaf_size=100, tol=1e-2)
+    corner, radius = h.root()
+    assert radius == dev["radius"]
+    np.testing.assert_array_equal(corner, dev["corner"])
+    np.testing.assert_array_equal(h.perm(), dev["perm"])
+    assert h.n_node == dev["n_node"] and h.max_level == dev["max_level"]
+    on = h.nodes()
+    for k in on:
+        np.testing.assert_array_equal(on[k], dev["nodes"][k], err_msg=k)
+    fp, fi, np_, ni = h.lists()
+    np.testing.assert_array_equal(fp, dev["far_ptr"])
+    np.testing.assert_array_equal(fi, dev["far_idx"])
+    np.testing.assert_array_equal(np_, dev["near_ptr"])
+    np.testing.assert_array_equal(ni, dev["near_idx"])
+
+
+@pytest.mark.parametrize("n_iter", [20, 100, 300, 1000])
+def test_h2_force_within_tolerance(mid, n_iter):
+    X, G, P, _ = mid
+    Y = _evolved(P, n_iter, 2).astype(np.float32).astype(np.float64)
+    eng = Engine(P, Y, n_iter=1)
+    assert eng.rebuild() == 0
+    F, Z = eng.repulsive(Y)
+    s, v = O.exact_sv(Y)
+    Ze, Fe = O.z_force(Y, s, v)
+    err = rel2(F, Fe)
+    print(f"iter {n_iter}: force rel {err:.3e}, Z rel {abs(Z - Ze) / Ze:.3e}, ranks max {eng.h2()['ranks'].max()}")
+    assert err <= 1e-2
+    assert abs(Z - Ze) <= 1e-2 * Ze
+
+
+def test_attractive_matches_oracle(mid):
+    from tsne_h2pack._backend import scipy_csr_to_c_sparse_matrix
+    X, G, P, _ = mid
+    Y = _evolved(P, 50, 3)
+    eng = Engine(P, Y, n_iter=1)
+    grad = np.zeros_like(Y)
+    Pc = scipy_csr_to_c_sparse_matrix(P, eng.lib)
+    eng.lib.compute_attractive_forces(ctypes.cast(Pc, ctypes.c_void_p), np.ascontiguousarray(Y), 2, Y.shape[1],
+                                      12.0, grad, 1)
+    eng.lib.sparse_matrix_destroy(Pc)
+    ref = O.attractive(P, Y, 12.0)
+    assert rel(grad, ref) < 1e-5
+
+
+def test_short_trajectory_matches_oracle(mid):
+    """Full schedule for 29 iterations (rebuilds every iteration, force from the H2 matrix)."""
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 2, 4)
+    eng = Engine(P, Y0, n_iter=29)
+    eng.run_all()
+    Yo, klo = O.run(P, Y0, n_iter=29)
+    r = rel(eng.embedding(), Yo)
+    print("29-iteration rel", r, eng.kl(), klo)
+    assert r < 5e-2
+    assert abs(eng.kl() - klo) < 1e-2 * abs(klo)
+
+
+def test_renumbering_is_transparent(mid, monkeypatch):
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 2, 8)
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TSNE_REORDER", flag)
+        eng = Engine(P, Y0, n_iter=34)
+        eng.run_all()
+        out[flag] = eng.embedding()
+        eng.close()
+    assert rel(out["1"], out["0"]) < 1e-3
+
+
+def test_deterministic(mid):
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 2, 9)
+    a = Engine(P, Y0, n_iter=40); a.run_all()
+    b = Engine(P, Y0, n_iter=40); b.run_all()
+    np.testing.assert_array_equal(a.embedding(), b.embedding())
+
+
+def test_full_run_quality():
+    """C1-shaped run (10K x 50, 10 clusters, k = 90, perplexity 30, 1000 iterations): KL within
+    1% of the oracle's run and 30-NN preservation within 0.5 points."""
+    X, G, P, _ = problem(10000, seed=0)
+    Y0 = O.init_embedding(P.shape[0], 2, 0)
+    eng = Engine(P, Y0, n_iter=1000)
+    eng.run_all()
+    Yd, kld = eng.embedding(), eng.kl()
+    Yo, klo = O.run(P, Y0, n_iter=1000)
+    pd, po = knn_preservation(X, Yd.T), knn_preservation(X, Yo.T)
+    print(f"KL device {kld:.5f} oracle {klo:.5f}; 30-NN device {pd:.4f} oracle {po:.4f}")
+    assert abs(kld - klo) <= 0.01 * klo
+    assert abs(pd - po) <= 0.005
+
+
+def test_nonfinite_embedding_is_rejected(mid):
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 2, 1)
+    Y0[0, 7] = np.nan
+    with pytest.raises(RuntimeError):
+        Engine(P, Y0, n_iter=5)
+
+
+def test_python_api_precomputed_matches_euclidean():
+    """The precomputed-graph path equals the feature path (reference test_tsne.py:765-811)."""
+    from tsne_h2pack import TSNE
+    X, G, P, _ = problem(3000, seed=5, dim=20)
+    kw = dict(n_components=2, perplexity=30, max_iter=40, init="random", random_state=3, knn_method="exact")
+    Ya = TSNE(**kw).fit_transform(X)
+    Yb = TSNE(metric="precomputed", **kw).fit_transform(G)
+    np.testing.assert_array_equal(Ya, Yb)

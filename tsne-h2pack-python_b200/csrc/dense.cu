@@ -1,0 +1,598 @@
+// Per-point and per-row kernels of the optimisation loop: the attractive CSR pass fused
+// with the gains/momentum update, centring, the exact O(N^2) repulsion, the Z identity and
+// force assembly, the KL divergence, point renumbering and the perplexity calibration.
+//
+// Reference counterparts (paths within the reference project):
+//   attractive pass ............ src/tsne_attr_2d.h:22-67, src/tsne_h2pack.c:199-356
+//   update + centring .......... src/tsne_h2pack.c:1942-1984
+//   exact repulsion ............ src/tsne_h2pack.c:404-491
+//   Z identity + force ......... src/tsne_h2pack.c:538-627
+//   KL ......................... src/tsne_h2pack.c:1870-1895
+//   renumbering ................ src/tsne_reorder.c:112-167
+//   perplexity calibration ..... src/tsne_utils.c:952-1105
+#include <math.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace tsne {
+
+namespace {
+
+template <int D> using Vec = typename Dim<D>::vec;
+
+template <int D>
+__device__ __forceinline__ Vec<D> vzero()
+{
+    Vec<D> v;
+    if constexpr (D == 2) v = make_float2(0.f, 0.f);
+    else v = make_float4(0.f, 0.f, 0.f, 0.f);
+    return v;
+}
+
+// Streamed P entries: read once per pass, kept out of L1 so Y stays cached.
+__device__ __forceinline__ int4 ld_stream_i4(const int *p)
+{
+    return __ldcs(reinterpret_cast<const int4 *>(p));
+}
+__device__ __forceinline__ float4 ld_stream_f4(const float *p)
+{
+    return __ldcs(reinterpret_cast<const float4 *>(p));
+}
+
+template <int D>
+__device__ __forceinline__ void attr_acc(const Vec<D> &yi, const Vec<D> *__restrict__ Y, int c, float p,
+                                         float (&a)[D])
+{
+    const Vec<D> yj = __ldg(Y + c);
+    float df[D], r2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; k++) { df[k] = vget(yi, k) - vget(yj, k); r2 = fmaf(df[k], df[k], r2); }
+    const float q = p * fast_rcp(1.0f + r2);
+#pragma unroll
+    for (int k = 0; k < D; k++) a[k] = fmaf(q, df[k], a[k]);
+}
+
+// Warp-per-row attractive sum over a row padded to a multiple of 4 entries; every lane
+// reads 4 column indices and 4 values with two 128-bit loads per step.
+template <int D>
+__device__ __forceinline__ void row_attr(int b, int e, int lane, const Vec<D> &yi, const int *__restrict__ col,
+                                         const float *__restrict__ val, const Vec<D> *__restrict__ Y,
+                                         float (&a)[D])
+{
+    for (int base = b + 4 * lane; base < e; base += 128) {
+        const int4 c4 = ld_stream_i4(col + base);
+        const float4 p4 = ld_stream_f4(val + base);
+        attr_acc<D>(yi, Y, c4.x, p4.x, a);
+        attr_acc<D>(yi, Y, c4.y, p4.y, a);
+        attr_acc<D>(yi, Y, c4.z, p4.z, a);
+        attr_acc<D>(yi, Y, c4.w, p4.w, a);
+    }
+#pragma unroll
+    for (int k = 0; k < D; k++) a[k] = warp_sum(a[k]);
+}
+
+// Block-wide FP64 reduction of per-warp values held by lane 0 of each warp, summed in
+// warp order; the result is valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum_warps(double (&v)[NV], double *out)
+{
+    __shared__ double sh[ROW_BLOCK / 32][NV];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < NV; k++) sh[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NV; k++) {
+            double s = 0.0;
+            for (int ww = 0; ww < ROW_BLOCK / 32; ww++) s += sh[ww][k];
+            out[k] = s;
+        }
+    }
+}
+
+// Fixed-order sum of `count` per-block partials (stride NV) by one block; result in sh_out.
+template <int NV>
+__device__ __forceinline__ void reduce_partials(const double *__restrict__ part, int count, double *sh_out)
+{
+    __shared__ double sh[RED_BLOCK][NV];
+    double acc[NV];
+    for (int k = 0; k < NV; k++) acc[k] = 0.0;
+    for (int b = threadIdx.x; b < count; b += blockDim.x)
+        for (int k = 0; k < NV; k++) acc[k] += part[(size_t)b * NV + k];
+    for (int k = 0; k < NV; k++) sh[threadIdx.x][k] = acc[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int k = 0; k < NV; k++) sh[threadIdx.x][k] += sh[threadIdx.x + s][k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NV; k++) sh_out[k] = sh[0][k];
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------
+// Attractive force + gains / momentum update (reference tsne_h2pack.c:1942-1968):
+//   g = 4 exag sum_j p_ij (y_i - y_j) / (1 + |y_i - y_j|^2) - F_rep
+//   gain: +0.2 if uY * g < 0 else * 0.8, floor 0.01; uY = mom uY - lr gain g; Y += uY
+// Ynext is a separate buffer because other warps still gather the old Y.
+// ---------------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+              float exag4, float mom, float lr, double *__restrict__ partials)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * (ROW_BLOCK / 32) + (threadIdx.x >> 5);
+    const int nwarp = gridDim.x * (ROW_BLOCK / 32);
+    const int use_rep = (rep != nullptr) ? *rep_flag : 0;
+    double acc[D];
+    for (int k = 0; k < D; k++) acc[k] = 0.0;
+    for (int i = warp; i < n; i += nwarp) {
+        const Vec<D> yi = Y[i];
+        float a[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) a[k] = 0.f;
+        row_attr<D>(rp[i], rp[i + 1], lane, yi, col, val, Y, a);
+        if (lane == 0) {
+            const Vec<D> r = use_rep ? rep[i] : vzero<D>();
+            Vec<D> u = uY[i], g = gains[i], yn = yi;
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                const float gk = exag4 * a[k] - vget(r, k);
+                const float uk = vget(u, k);
+                float gain = (uk * gk < 0.f) ? vget(g, k) + 0.2f : vget(g, k) * 0.8f;
+                gain = fmaxf(gain, 0.01f);
+                const float un = mom * uk - lr * (gk * gain);
+                vset(g, k, gain);
+                vset(u, k, un);
+                vset(yn, k, vget(yi, k) + un);
+                acc[k] += (double)vget(yn, k);
+            }
+            uY[i] = u;
+            gains[i] = g;
+            Yn[i] = yn;
+        }
+    }
+    block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
+}
+
+// Centring (reference tsne_h2pack.c:1978-1984): Y = Ynext - mean(Ynext), the mean summed
+// in FP64 from the update's fixed per-block partials, identically in every block.
+template <int D>
+__global__ void __launch_bounds__(RED_BLOCK)
+k_center(int n, const Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ Y, const double *__restrict__ partials,
+         DevScalars *sc)
+{
+    __shared__ double mean[D];
+    reduce_partials<D>(partials, ROW_GRID, mean);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < D; k++) mean[k] /= (double)n;
+        if (blockIdx.x == 0)
+            for (int k = 0; k < D; k++) sc->mean[k] = mean[k];
+    }
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Vec<D> v = Yn[i];
+#pragma unroll
+        for (int k = 0; k < D; k++) vset(v, k, (float)((double)vget(v, k) - mean[k]));
+        Y[i] = v;
+    }
+}
+
+// Exact off-diagonal sums s_i = sum_{j != i} K_ij, v_i = sum_{j != i} K_ij y_j
+// (reference tsne_h2pack.c:404-491): one thread per target, sources staged through
+// shared memory 256 at a time, FP32 per tile and FP64 across tiles.
+template <int D>
+__global__ void __launch_bounds__(256)
+k_exact_sv(int n, const Vec<D> *__restrict__ Y, float *__restrict__ s, Vec<D> *__restrict__ v)
+{
+    __shared__ Vec<D> sh[256];
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    const Vec<D> yi = (i < n) ? Y[i] : vzero<D>();
+    double S = 0.0, V[D];
+    for (int k = 0; k < D; k++) V[k] = 0.0;
+    for (int base = 0; base < n; base += 256) {
+        __syncthreads();
+        if (base + (int)threadIdx.x < n) sh[threadIdx.x] = Y[base + threadIdx.x];
+        __syncthreads();
+        const int cnt = min(256, n - base);
+        float ts = 0.f, tv[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) tv[k] = 0.f;
+        for (int j = 0; j < cnt; j++) {
+            const Vec<D> yj = sh[j];
+            float w = rkernel(dist2(yi, yj));
+            w = (base + j == i) ? 0.f : w;
+            ts += w;
+#pragma unroll
+            for (int k = 0; k < D; k++) tv[k] = fmaf(w, vget(yj, k), tv[k]);
+        }
+        S += ts;
+        for (int k = 0; k < D; k++) V[k] += tv[k];
+    }
+    if (i < n) {
+        s[i] = (float)S;
+        Vec<D> o = vzero<D>();
+        for (int k = 0; k < D; k++) vset(o, k, (float)V[k]);
+        v[i] = o;
+    }
+}
+
+// Z identity (reference tsne_h2pack.c:558-590): Z = sum s + 2 sum |y|^2 s - 2 sum y.v,
+// three FP64 sums over fixed blocks.
+template <int D>
+__global__ void __launch_bounds__(RED_BLOCK)
+k_z_part(int n, const Vec<D> *__restrict__ Yp, const float *__restrict__ s, const Vec<D> *__restrict__ v,
+         double *__restrict__ partials)
+{
+    double t[3] = {0.0, 0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> y = Yp[i], vv = v[i];
+        double yy = 0.0, yv = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            const double yk = vget(y, k);
+            yy += yk * yk;
+            yv += yk * (double)vget(vv, k);
+        }
+        t[0] += s[i];
+        t[1] += yy * s[i];
+        t[2] += yv;
+    }
+    __shared__ double sh[RED_BLOCK][3];
+    for (int k = 0; k < 3; k++) sh[threadIdx.x][k] = t[k];
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st)
+            for (int k = 0; k < 3; k++) sh[threadIdx.x][k] += sh[threadIdx.x + st][k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 3; k++) partials[(size_t)blockIdx.x * 3 + k] = sh[0][k];
+}
+
+// Force assembly (reference tsne_h2pack.c:604-627): F_i = (4/Z)(y_i s_i - v_i), written in
+// point order (perm maps tree positions to points). On the H2 path a non-positive or
+// non-finite Z skips the force, as the reference does.
+template <int D>
+__global__ void __launch_bounds__(RED_BLOCK)
+k_force(int n, const Vec<D> *__restrict__ Yp, const float *__restrict__ s, const Vec<D> *__restrict__ v,
+        const int *__restrict__ perm, Vec<D> *__restrict__ F, DevScalars *sc,
+        const double *__restrict__ partials, int nblk, int h2_path, int keep_rep)
+{
+    __shared__ double tz[3];
+    reduce_partials<3>(partials, nblk, tz);
+    const double Z = tz[0] + 2.0 * tz[1] - 2.0 * tz[2];
+    const bool ok = !h2_path || (Z > 0.0 && isfinite(Z));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->Z = ok ? Z : 1.0;
+        sc->force_ok = ok ? 1 : 0;
+        sc->bad_z = ok ? 0 : 1;
+        if (ok && keep_rep) { sc->rep_valid = 1; sc->rep_Z = Z; }
+    }
+    if (!ok) return;
+    const double c = 4.0 / Z;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> y = Yp[i], vv = v[i];
+        const double si = s[i];
+        Vec<D> f = vzero<D>();
+#pragma unroll
+        for (int k = 0; k < D; k++) vset(f, k, (float)(c * ((double)vget(y, k) * si - (double)vget(vv, k))));
+        F[perm ? perm[i] : i] = f;
+    }
+}
+
+// KL(P || Q) of the exaggerated P with q_ij = 1 / ((1 + |y_i - y_j|^2) Z)
+// (reference tsne_h2pack.c:1870-1895), FP64 per entry.
+template <int D>
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_kl(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+     const Vec<D> *__restrict__ Y, double exag, const DevScalars *__restrict__ sc, double *__restrict__ partials)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * (ROW_BLOCK / 32) + (threadIdx.x >> 5);
+    const int nwarp = gridDim.x * (ROW_BLOCK / 32);
+    const double Z = sc->Z;
+    double acc[1] = {0.0};
+    for (int i = warp; i < n; i += nwarp) {
+        const Vec<D> yi = Y[i];
+        double r = 0.0;
+        for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) {
+            const double p = (double)val[e] * exag;
+            const Vec<D> yj = Y[col[e]];
+            double r2 = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; k++) { const double df = (double)vget(yi, k) - (double)vget(yj, k); r2 += df * df; }
+            const double q = 1.0 / ((1.0 + r2) * Z);
+            if (p > 1e-12 && q > 1e-12) r += p * log(p / q);
+        }
+        r = warp_sum(r);
+        if (lane == 0) acc[0] += r;
+    }
+    block_sum_warps<1>(acc, partials + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_BLOCK) k_kl_final(const double *__restrict__ partials, int nblk, DevScalars *sc)
+{
+    __shared__ double out[1];
+    reduce_partials<1>(partials, nblk, out);
+    if (threadIdx.x == 0) sc->kl = out[0];
+}
+
+// grad (SoA double, reference layout) += scale * attractive sums
+template <int D>
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_attr_only(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+            const Vec<D> *__restrict__ Y, double scale, double *__restrict__ grad)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * (ROW_BLOCK / 32) + (threadIdx.x >> 5);
+    const int nwarp = gridDim.x * (ROW_BLOCK / 32);
+    for (int i = warp; i < n; i += nwarp) {
+        float a[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) a[k] = 0.f;
+        row_attr<D>(rp[i], rp[i + 1], lane, Y[i], col, val, Y, a);
+        if (lane == 0)
+            for (int k = 0; k < D; k++) grad[(size_t)k * n + i] += scale * (double)a[k];
+    }
+}
+
+template <int D>
+__global__ void k_soa_to_vec(int n, const double *__restrict__ soa, Vec<D> *__restrict__ v)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Vec<D> o = vzero<D>();
+        for (int k = 0; k < D; k++) vset(o, k, (float)soa[(size_t)k * n + i]);
+        v[i] = o;
+    }
+}
+
+template <int D>
+__global__ void k_vec_to_soa(int n, const Vec<D> *__restrict__ v, double *__restrict__ soa)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> x = v[i];
+        for (int k = 0; k < D; k++) soa[(size_t)k * n + i] = (double)vget(x, k);
+    }
+}
+
+template <int D>
+__global__ void k_fill_vec(int n, Vec<D> *__restrict__ v, float value)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Vec<D> o = vzero<D>();
+        for (int k = 0; k < D; k++) vset(o, k, value);
+        v[i] = o;
+    }
+}
+
+template <int D>
+__global__ void k_permute_vec(int n, const int *__restrict__ ord, const Vec<D> *__restrict__ src,
+                              Vec<D> *__restrict__ dst)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = src[ord[i]];
+}
+
+__global__ void k_permute_int(int n, const int *__restrict__ ord, const int *__restrict__ src,
+                              int *__restrict__ dst, int identity_src)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = identity_src ? ord[i] : src[ord[i]];
+}
+
+__global__ void k_invert_perm(int n, const int *__restrict__ ord, int *__restrict__ inv)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) inv[ord[i]] = i;
+}
+
+__global__ void k_row_len(int n, const int *__restrict__ ord, const int *__restrict__ rp, int *__restrict__ len)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = ord[k];
+        len[k] = rp[i + 1] - rp[i];
+    }
+}
+
+// Renumbered rows (reference tsne_reorder.c:112-167): new row k is old row ord[k] with
+// columns mapped through inv; the rows are sorted by column afterwards.
+__global__ void k_row_copy(int n, const int *__restrict__ ord, const int *__restrict__ inv,
+                           const int *__restrict__ rp_old, const int *__restrict__ col_old,
+                           const float *__restrict__ val_old, const int *__restrict__ rp_new,
+                           int *__restrict__ col_new, float *__restrict__ val_new)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (int k = warp; k < n; k += nwarp) {
+        const int i = ord[k], b = rp_old[i], len = rp_old[i + 1] - b, o = rp_new[k];
+        for (int e = lane; e < len; e += 32) {
+            col_new[o + e] = inv[col_old[b + e]];
+            val_new[o + e] = val_old[b + e];
+        }
+    }
+}
+
+// Conditional P_j|i by bisection on beta over min-shifted squared distances, FP64
+// (reference tsne_utils.c:952-1005): one warp per row; the search state is uniform
+// across the warp and every sum is a warp reduction.
+__global__ void __launch_bounds__(256)
+k_pcal(int n, const int *__restrict__ indptr, const double *__restrict__ dist, double perplexity,
+       double *__restrict__ out)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarp = (gridDim.x * blockDim.x) >> 5;
+    const double target = log(perplexity);
+    for (int i = warp; i < n; i += nwarp) {
+        const int b = indptr[i], k = indptr[i + 1] - b;
+        if (k <= 0) continue;
+        double dmin = INFINITY;
+        for (int j = lane; j < k; j += 32) { const double d = dist[b + j]; dmin = fmin(dmin, d * d); }
+        for (int o = 16; o > 0; o >>= 1) dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+        double beta = 1.0, lo = 0.0, hi = 0.0, sp = 1.0;
+        bool have_lo = false, have_hi = false;
+        double beta_eval = beta;
+        for (int it = 0; it < 200; it++) {
+            double a = 0.0, c = 0.0;
+            for (int j = lane; j < k; j += 32) {
+                const double d = dist[b + j];
+                const double dd = d * d - dmin;
+                const double p = exp(-beta * dd);
+                a += p;
+                c += dd * p;
+            }
+            a = warp_sum(a);
+            c = warp_sum(c);
+            sp = a;
+            beta_eval = beta;
+            const double H = log(a) + beta * c / a;
+            const double diff = H - target;
+            if (fabs(diff) < 1e-5) break;
+            if (diff > 0.0) { lo = beta; have_lo = true; beta = have_hi ? 0.5 * (beta + hi) : 2.0 * beta; }
+            else            { hi = beta; have_hi = true; beta = have_lo ? 0.5 * (beta + lo) : 0.5 * beta; }
+        }
+        const double inv = 1.0 / sp;
+        for (int j = lane; j < k; j += 32) {
+            const double d = dist[b + j];
+            out[b + j] = exp(-beta_eval * (d * d - dmin)) * inv;
+        }
+    }
+}
+
+constexpr int EW_BLOCK = 256;
+inline int ew_grid(int n) { int g = ceil_div(n, EW_BLOCK); return g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------
+template <int D>
+void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
+                        const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
+                        const int *rep_flag, float exag4, float mom, float lr, double *partials)
+{
+    k_attr_update<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
+}
+
+template <int D>
+void launch_center(cudaStream_t st, int n, const void *Ynext, void *Ycur, const double *partials,
+                   DevScalars *sc, const void *, double *)
+{
+    k_center<D><<<ew_grid(n), RED_BLOCK, 0, st>>>(n, (const Vec<D> *)Ynext, (Vec<D> *)Ycur, partials, sc);
+}
+
+template <int D>
+void launch_exact_sv(cudaStream_t st, int n, const void *Y, float *s, void *v)
+{
+    k_exact_sv<D><<<ceil_div(n, 256), 256, 0, st>>>(n, (const Vec<D> *)Y, s, (Vec<D> *)v);
+}
+
+template <int D>
+void launch_z_force(cudaStream_t st, int n, const void *Ypts, const float *s, const void *v,
+                    const int *perm, void *rep, DevScalars *sc, double *partials, int h2_path,
+                    int keep_rep)
+{
+    const int nblk = 148 * 2;
+    k_z_part<D><<<nblk, RED_BLOCK, 0, st>>>(n, (const Vec<D> *)Ypts, s, (const Vec<D> *)v, partials);
+    k_force<D><<<ew_grid(n), RED_BLOCK, 0, st>>>(n, (const Vec<D> *)Ypts, s, (const Vec<D> *)v, perm,
+                                                 (Vec<D> *)rep, sc, partials, nblk, h2_path, keep_rep);
+}
+
+template <int D>
+void launch_kl(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
+               const void *Y, double exag, DevScalars *sc, double *partials)
+{
+    k_kl<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, rp, col, val, (const Vec<D> *)Y, exag, sc, partials);
+    k_kl_final<<<1, RED_BLOCK, 0, st>>>(partials, ROW_GRID, sc);
+}
+
+template <int D>
+void launch_attr_only(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
+                      const void *Y, double scale, double *grad_soa)
+{
+    k_attr_only<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, rp, col, val, (const Vec<D> *)Y, scale, grad_soa);
+}
+
+template <int D>
+void launch_soa_to_vec(cudaStream_t st, int n, const double *soa, void *vec)
+{
+    k_soa_to_vec<D><<<ew_grid(n), EW_BLOCK, 0, st>>>(n, soa, (Vec<D> *)vec);
+}
+
+template <int D>
+void launch_vec_to_soa(cudaStream_t st, int n, const void *vec, double *soa)
+{
+    k_vec_to_soa<D><<<ew_grid(n), EW_BLOCK, 0, st>>>(n, (const Vec<D> *)vec, soa);
+}
+
+template <int D>
+void launch_fill_vec(cudaStream_t st, int n, void *vec, float value)
+{
+    k_fill_vec<D><<<ew_grid(n), EW_BLOCK, 0, st>>>(n, (Vec<D> *)vec, value);
+}
+
+template <int D>
+void launch_permute_vec(cudaStream_t st, int n, const int *ord, const void *src, void *dst)
+{
+    k_permute_vec<D><<<ew_grid(n), EW_BLOCK, 0, st>>>(n, ord, (const Vec<D> *)src, (Vec<D> *)dst);
+}
+
+void launch_permute_int(cudaStream_t st, int n, const int *ord, const int *src, int *dst, int identity_src)
+{
+    k_permute_int<<<ew_grid(n), EW_BLOCK, 0, st>>>(n, ord, src, dst, identity_src);
+}
+
+void launch_invert_perm(cudaStream_t st, int n, const int *ord, int *inv)
+{
+    k_invert_perm<<<ew_grid(n), EW_BLOCK, 0, st>>>(n, ord, inv);
+}
+
+void launch_row_len(cudaStream_t st, int n, const int *ord, const int *rp_old, int *len_new)
+{
+    k_row_len<<<ew_grid(n), EW_BLOCK, 0, st>>>(n, ord, rp_old, len_new);
+}
+
+void launch_row_copy(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
+                     const int *col_old, const float *val_old, const int *rp_new, int *col_new,
+                     float *val_new)
+{
+    k_row_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, ord, inv, rp_old, col_old, val_old, rp_new, col_new, val_new);
+}
+
+void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist, double perplexity,
+                 double *out)
+{
+    k_pcal<<<ROW_GRID, 256, 0, st>>>(n, indptr, dist, perplexity, out);
+}
+
+#define TSNE_INST(D)                                                                              \
+    template void launch_attr_update<D>(cudaStream_t, int, const int *, const int *, const float *,  \
+                                        const void *, void *, void *, void *, const void *,          \
+                                        const int *, float, float, float, double *);                 \
+    template void launch_center<D>(cudaStream_t, int, const void *, void *, const double *,         \
+                                   DevScalars *, const void *, double *);                            \
+    template void launch_exact_sv<D>(cudaStream_t, int, const void *, float *, void *);             \
+    template void launch_z_force<D>(cudaStream_t, int, const void *, const float *, const void *,   \
+                                    const int *, void *, DevScalars *, double *, int, int);          \
+    template void launch_kl<D>(cudaStream_t, int, const int *, const int *, const float *,          \
+                               const void *, double, DevScalars *, double *);                       \
+    template void launch_attr_only<D>(cudaStream_t, int, const int *, const int *, const float *,   \
+                                      const void *, double, double *);                              \
+    template void launch_soa_to_vec<D>(cudaStream_t, int, const double *, void *);                  \
+    template void launch_vec_to_soa<D>(cudaStream_t, int, const void *, double *);                  \
+    template void launch_fill_vec<D>(cudaStream_t, int, void *, float);                             \
+    template void launch_permute_vec<D>(cudaStream_t, int, const int *, const void *, void *);
+
+TSNE_INST(2)
+TSNE_INST(3)
+
+}  // namespace tsne

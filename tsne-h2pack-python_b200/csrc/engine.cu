@@ -1,0 +1,1017 @@
+// The optimisation engine behind the C ABI (include/tsne_h2pack.h): one workspace per
+// embedding, all state resident on the current CUDA device, the reference's schedule
+// (src/tsne_h2pack.c:1652-2102) driven from the host with one stream per workspace.
+#include <cub/cub.cuh>
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <algorithm>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "devbuf.h"
+#include "h2.h"
+#include "kernels.h"
+#include "../../include/tsne_h2pack.h"
+
+using namespace tsne;
+
+namespace {
+
+int env_int(const char *name, int dflt)
+{
+    const char *v = getenv(name);
+    return (v != nullptr && *v != '\0') ? atoi(v) : dflt;
+}
+
+double wall_sec()
+{
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+// CSR rows padded to a multiple of 4 entries (column = the row itself, value 0) so that the
+// attractive pass reads 4 entries per 128-bit load.
+__global__ void k_pad_len(int n, const int *__restrict__ rp, int *__restrict__ len)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        len[i] = (rp[i + 1] - rp[i] + 3) & ~3;
+}
+__global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ pv,
+                           const int *__restrict__ rpp, int *__restrict__ col, float *__restrict__ val)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < n; i += nwarp) {
+        const int b = rp[i], len = rp[i + 1] - b, o = rpp[i], plen = rpp[i + 1] - o;
+        for (int e = lane; e < plen; e += 32) {
+            col[o + e] = e < len ? ci[b + e] : i;
+            val[o + e] = e < len ? (float)pv[b + e] : 0.f;
+        }
+    }
+}
+__global__ void k_conv_check(int n, const float *__restrict__ Y, const float *__restrict__ Yprev, int d,
+                             int vec_stride, double *__restrict__ out_max)
+{
+    __shared__ double sh[256];
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = 0; k < d; k++) {
+            const double df = (double)Y[(size_t)i * vec_stride + k] - (double)Yprev[(size_t)i * vec_stride + k];
+            s += df * df;
+        }
+        m = fmax(m, sqrt(s));
+    }
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out_max[blockIdx.x] = sh[0];
+}
+
+}  // namespace
+
+struct tsne_workspace {
+    tsne_params_t params{};
+    std::string prof_file;
+    int n = 0, d = 0, pt_dim = 0;
+    double lr = 200.0;
+    sparse_matrix_t *P = nullptr;   // host P (owned, as in the reference)
+    size_t vbytes = 0;              // bytes per point of the device vectors
+
+    cudaStream_t st = nullptr;
+    DevBuf<int> rp, col, rp2, col2, len, inv, order, order2;
+    DevBuf<float> val, val2;
+    DevBuf<unsigned char> Y, Yn, uY, gains, rep, frc, tmpv, Yconv;
+    DevBuf<float> s;
+    DevBuf<unsigned char> v;
+    DevBuf<DevScalars> sc;
+    HostPinned<DevScalars> hsc;
+    DevBuf<double> part, zpart, klpart, convpart;
+    DevBuf<unsigned char> cub_tmp;
+    std::unique_ptr<H2Matrix> h2;
+    bool h2_valid = false;
+    bool has_order = false;
+    bool rep_valid_host = false;
+    int next_reorder = 0;
+    int n_rebuild = 0;
+    long long n_launch = 0;
+    double kl = 0.0;
+    int convergence_count = 0, converged = 0;
+    std::vector<double> iter_times;
+    profiling_data_t *prof = nullptr;
+};
+
+struct tsne_h2_matrix {
+    tsne_workspace *ws;
+};
+
+namespace {
+
+template <int D> size_t vec_bytes() { return sizeof(typename Dim<D>::vec); }
+
+void upload_P(tsne_workspace *ws)
+{
+    const int n = ws->n, nnz = ws->P->row_ptr[n];
+    cudaStream_t st = ws->st;
+    DevBuf<int> rp0, ci0;
+    DevBuf<double> pv0;
+    rp0.exact(n + 1);
+    ci0.exact(std::max(nnz, 1));
+    pv0.exact(std::max(nnz, 1));
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(rp0.p, ws->P->row_ptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+    if (nnz > 0) {
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(ci0.p, ws->P->col_idx, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(pv0.p, ws->P->values, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+    }
+    ws->len.exact(n + 1);
+    ws->rp.exact(n + 2);
+    k_pad_len<<<ceil_div(n, 256), 256, 0, st>>>(n, rp0.p, ws->len.p);
+    TSNE_CUDA_CHECK(cudaMemsetAsync(ws->rp.p, 0, sizeof(int), st));
+    size_t bytes = 0;
+    TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(nullptr, bytes, ws->len.p, ws->rp.p + 1, n, st));
+    ws->cub_tmp.ensure(bytes + 256);
+    bytes = ws->cub_tmp.cap;
+    TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(ws->cub_tmp.p, bytes, ws->len.p, ws->rp.p + 1, n, st));
+    int padded = 0;
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(&padded, ws->rp.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    ws->col.exact(std::max(padded, 4));
+    ws->val.exact(std::max(padded, 4));
+    k_pad_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, rp0.p, ci0.p, pv0.p, ws->rp.p, ws->col.p, ws->val.p);
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    ws->n_launch += 3;
+}
+
+template <int D>
+void soa_to_device(tsne_workspace *ws, const double *soa_host, void *dst)
+{
+    DevBuf<double> tmp;
+    tmp.exact((size_t)ws->n * D);
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(tmp.p, soa_host, sizeof(double) * ws->n * D, cudaMemcpyHostToDevice, ws->st));
+    launch_soa_to_vec<D>(ws->st, ws->n, tmp.p, dst);
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+}
+
+void upload_soa(tsne_workspace *ws, const double *soa_host, void *dst)
+{
+    if (ws->d == 2) soa_to_device<2>(ws, soa_host, dst);
+    else soa_to_device<3>(ws, soa_host, dst);
+}
+
+// device vec -> host SoA double, in the caller's point order
+void download_soa(tsne_workspace *ws, const void *src, double *out)
+{
+    const int n = ws->n, d = ws->d;
+    DevBuf<double> tmp;
+    tmp.exact((size_t)n * d);
+    if (d == 2) launch_vec_to_soa<2>(ws->st, n, src, tmp.p);
+    else launch_vec_to_soa<3>(ws->st, n, src, tmp.p);
+    std::vector<double> h((size_t)n * d);
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(h.data(), tmp.p, sizeof(double) * n * d, cudaMemcpyDeviceToHost, ws->st));
+    std::vector<int> ord;
+    if (ws->has_order) {
+        ord.resize(n);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(ord.data(), ws->order.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ws->st));
+    }
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < n; j++) out[(size_t)k * n + (ws->has_order ? ord[j] : j)] = h[(size_t)k * n + j];
+}
+
+// Rebuild the H2 matrix for the current embedding (reference update_h2_matrix,
+// src/tsne_h2pack.c:772-953). 0 ok (h2_valid tells whether an H2 matrix exists), -1 failure.
+int rebuild_h2(tsne_workspace *ws)
+{
+    if (ws->n < 2000) { ws->h2_valid = false; return 0; }
+    if (!ws->h2) ws->h2 = make_h2_matrix(ws->d, ws->n, ws->st);
+    const int leaf = ws->params.h2_leaf_size > 0 ? ws->params.h2_leaf_size : 100;
+    const double tol = ws->params.h2_tol > 0.0 ? ws->params.h2_tol : 1e-6;
+    const long long l0 = ws->h2->launches();
+    const int rc = ws->h2->build(ws->Y.p, leaf, tol);
+    ws->n_launch += ws->h2->launches() - l0;
+    if (rc < 0) {
+        fprintf(stderr, "ERROR: Y contains NaN or Inf!\n");
+        ws->h2_valid = false;
+        return -1;
+    }
+    ws->h2_valid = (rc == 0);
+    if (rc == 1 && (ws->params.verbose || ws->params.h2pack_print_level >= 1))
+        printf("  Skipping H2 approximation: shallow tree (max_level=%d <= 2), using direct O(N^2) sums\n",
+               ws->h2->stats().max_level);
+    if (ws->h2_valid && ws->params.h2pack_print_level >= 1) {
+        const H2Stats &s = ws->h2->stats();
+        printf("  H2 matrix: %d nodes, max level %d, far %d, near %d, rank max %d mean %.1f\n", s.n_node,
+               s.max_level, s.n_far, s.n_near, s.rank_max, s.rank_mean);
+    }
+    return 0;
+}
+
+template <int D>
+void renumber_impl(tsne_workspace *ws, const int *ord_dev)
+{
+    const int n = ws->n;
+    cudaStream_t st = ws->st;
+    ws->inv.exact(n);
+    ws->len.exact(n + 1);
+    ws->rp2.exact(n + 2);
+    launch_invert_perm(st, n, ord_dev, ws->inv.p);
+    launch_row_len(st, n, ord_dev, ws->rp.p, ws->len.p);
+    TSNE_CUDA_CHECK(cudaMemsetAsync(ws->rp2.p, 0, sizeof(int), st));
+    size_t bytes = 0;
+    TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(nullptr, bytes, ws->len.p, ws->rp2.p + 1, n, st));
+    ws->cub_tmp.ensure(bytes + 256);
+    bytes = ws->cub_tmp.cap;
+    TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(ws->cub_tmp.p, bytes, ws->len.p, ws->rp2.p + 1, n, st));
+    int total = 0;
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(&total, ws->rp.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    ws->col2.exact(std::max(total, 4));
+    ws->val2.exact(std::max(total, 4));
+    DevBuf<int> colu;
+    DevBuf<float> valu;
+    colu.exact(std::max(total, 4));
+    valu.exact(std::max(total, 4));
+    launch_row_copy(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, colu.p, valu.p);
+    size_t sb = 0;
+    TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(nullptr, sb, colu.p, ws->col2.p, valu.p, ws->val2.p, total,
+                                                         n, ws->rp2.p, ws->rp2.p + 1, st));
+    ws->cub_tmp.ensure(sb + 256);
+    sb = ws->cub_tmp.cap;
+    TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(ws->cub_tmp.p, sb, colu.p, ws->col2.p, valu.p, ws->val2.p,
+                                                         total, n, ws->rp2.p, ws->rp2.p + 1, st));
+    std::swap(ws->rp.p, ws->rp2.p); std::swap(ws->rp.cap, ws->rp2.cap);
+    std::swap(ws->col.p, ws->col2.p); std::swap(ws->col.cap, ws->col2.cap);
+    std::swap(ws->val.p, ws->val2.p); std::swap(ws->val.cap, ws->val2.cap);
+    ws->tmpv.exact(ws->vbytes * n);
+    DevBuf<unsigned char> *arrs[] = {&ws->Y, &ws->uY, &ws->gains, &ws->rep, ws->Yconv.p ? &ws->Yconv : nullptr};
+    for (DevBuf<unsigned char> *a : arrs) {
+        if (a == nullptr) continue;
+        launch_permute_vec<D>(st, n, ord_dev, a->p, ws->tmpv.p);
+        std::swap(a->p, ws->tmpv.p);
+        std::swap(a->cap, ws->tmpv.cap);
+    }
+    ws->order2.exact(n);
+    launch_permute_int(st, n, ord_dev, ws->has_order ? ws->order.p : nullptr, ws->order2.p, ws->has_order ? 0 : 1);
+    std::swap(ws->order.p, ws->order2.p);
+    std::swap(ws->order.cap, ws->order2.cap);
+    ws->has_order = true;
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    ws->n_launch += 14;
+}
+
+void renumber(tsne_workspace *ws, const int *ord_dev)
+{
+    if (ws->d == 2) renumber_impl<2>(ws, ord_dev);
+    else renumber_impl<3>(ws, ord_dev);
+}
+
+// exact O(N^2) sums + Z + force into ws->frc (reference tsne_h2pack.c:404-491)
+template <int D>
+void exact_force(tsne_workspace *ws)
+{
+    ws->s.exact(ws->n);
+    ws->v.exact(ws->vbytes * ws->n);
+    ws->frc.exact(ws->vbytes * ws->n);
+    launch_exact_sv<D>(ws->st, ws->n, ws->Y.p, ws->s.p, ws->v.p);
+    launch_z_force<D>(ws->st, ws->n, ws->Y.p, ws->s.p, ws->v.p, nullptr, ws->frc.p, ws->sc.p, ws->zpart.p, 0, 0);
+    ws->n_launch += 3;
+}
+
+bool next_reorder_due(tsne_workspace *ws, int iter, const int *iters, int n_reorder)
+{
+    return ws->next_reorder < n_reorder && iter >= iters[ws->next_reorder];
+}
+
+void stage_event(tsne_workspace *ws, std::vector<cudaEvent_t> &pool, size_t &used)
+{
+    if (used == pool.size()) {
+        cudaEvent_t e;
+        TSNE_CUDA_CHECK(cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    TSNE_CUDA_CHECK(cudaEventRecord(pool[used++], ws->st));
+}
+
+template <int D>
+int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
+{
+    const tsne_params_t &p = ws->params;
+    const int n = ws->n, n_iter = p.n_iter;
+    const int verbose = p.verbose, print_freq = p.print_freq > 0 ? p.print_freq : 50;
+    const int sklearn = p.sklearn_compatible;
+    const int rep_reuse = env_int("TSNE_REP_REUSE", 1) && n >= 2000;
+    int reorder_iters[16] = {30, 100, 250, 400, 600, 800};
+    int n_reorder = env_int("TSNE_REORDER", 1) ? 6 : 0;
+    const char *reorder_env = getenv("TSNE_REORDER_ITERS");
+    if (n_reorder > 0 && reorder_env != nullptr && *reorder_env != '\0') {
+        n_reorder = 0;
+        for (const char *c = reorder_env; *c != '\0' && n_reorder < 16;) {
+            reorder_iters[n_reorder++] = atoi(c);
+            while (*c != '\0' && *c != ',') c++;
+            if (*c == ',') c++;
+        }
+    }
+    const int h2_freq = p.h2_rebuild_freq > 0 ? p.h2_rebuild_freq : 10;
+    const bool never_h2 = h2_freq > 100000;
+    cudaStream_t st = ws->st;
+    const long long launch0 = ws->n_launch;
+    ws->n_rebuild = 0;
+
+    // profiling: events per stage, resolved at the end
+    const bool prof = ws->prof != nullptr;
+    std::vector<cudaEvent_t> evpool;
+    size_t evused = 0;
+    struct StageEv { int iter; int stage; size_t a, b; };
+    std::vector<StageEv> stages;
+
+    int ret = 0;
+    for (int iter = it_begin; iter < it_end; iter++) {
+        const double t_iter = wall_sec();
+        const double mom = iter >= p.momentum_switch_iter ? p.momentum : p.initial_momentum;
+        double exag;
+        if (sklearn) exag = iter < p.early_exag_iter ? p.early_exag : 1.0;
+        else if (iter < p.early_exag_iter) exag = p.early_exag;
+        else if (iter < p.early_exag_iter + 100) exag = p.early_exag - (p.early_exag - 1.0) * ((double)(iter - p.early_exag_iter) / 100.0);
+        else exag = 1.0;
+        double lr = ws->lr;
+        if (!sklearn && iter >= p.momentum_switch_iter) lr = ws->lr * pow(0.995, iter - p.momentum_switch_iter);
+
+        int eff = iter < 20 ? 1 : h2_freq;
+        if (iter >= 20 && iter < p.early_exag_iter && rep_reuse && p.h2_rebuild_freq_early > eff)
+            eff = p.h2_rebuild_freq_early;
+        bool rebuilt = (iter == 0);
+        const bool want = iter > 0 && iter % eff == 0;
+        if (n >= 2000 && want && !never_h2) {
+            size_t e0 = evused;
+            if (prof) stage_event(ws, evpool, evused);
+            if (next_reorder_due(ws, iter, reorder_iters, n_reorder) && ws->h2_valid) {
+                while (ws->next_reorder < n_reorder && iter >= reorder_iters[ws->next_reorder]) ws->next_reorder++;
+                renumber(ws, ws->h2->perm_device());
+            }
+            if (rebuild_h2(ws) != 0) {
+                fprintf(stderr, "ERROR: Failed to rebuild H2 matrix at iteration %d\n", iter);
+                ret = -1;
+                break;
+            }
+            rebuilt = true;
+            ws->n_rebuild++;
+            if (prof) { stage_event(ws, evpool, evused); stages.push_back({iter, 1, e0, evused - 1}); }
+        }
+
+        // repulsion: reuse, H2 product, or exact sums
+        const void *force = nullptr;
+        const int *flag = nullptr;
+        size_t e1 = evused;
+        if (prof) stage_event(ws, evpool, evused);
+        const bool reuse = rep_reuse && !rebuilt && ws->rep_valid_host;
+        if (reuse) {
+            force = ws->rep.p;
+            flag = &ws->sc.p->rep_valid;
+        } else if (ws->h2_valid && !never_h2) {
+            const long long l0 = ws->h2->launches();
+            ws->h2->product_force(ws->rep.p, ws->sc.p, ws->zpart.p, rep_reuse ? 1 : 0);
+            ws->n_launch += ws->h2->launches() - l0;
+            force = ws->rep.p;
+            flag = &ws->sc.p->force_ok;
+            if (rep_reuse) ws->rep_valid_host = true;
+        } else {
+            exact_force<D>(ws);
+            force = ws->frc.p;
+            flag = &ws->sc.p->force_ok;
+        }
+        if (prof && !reuse) { stage_event(ws, evpool, evused); stages.push_back({iter, 2, e1, evused - 1}); }
+
+        if (!sklearn && iter > p.momentum_switch_iter) {
+            if (reuse) TSNE_CUDA_CHECK(cudaMemcpyAsync(&ws->sc.p->Z, &ws->sc.p->rep_Z, sizeof(double), cudaMemcpyDeviceToDevice, st));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+            TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+            if (ws->hsc.p->Z < 10.0) {
+                if (verbose) printf("\n*** STOPPING: Z collapsed to %.3e (threshold: 10.0) ***\n", ws->hsc.p->Z);
+                break;
+            }
+        }
+        const bool want_kl = (verbose && iter % 50 == 0) || iter == n_iter - 1;
+        if (want_kl) {
+            if (reuse) TSNE_CUDA_CHECK(cudaMemcpyAsync(&ws->sc.p->Z, &ws->sc.p->rep_Z, sizeof(double), cudaMemcpyDeviceToDevice, st));
+            launch_kl<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, exag, ws->sc.p, ws->klpart.p);
+            ws->n_launch += 2;
+        }
+
+        size_t e2 = evused;
+        if (prof) stage_event(ws, evpool, evused);
+        launch_attr_update<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p, ws->uY.p, ws->gains.p,
+                              force, flag, (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
+        if (prof) { stage_event(ws, evpool, evused); stages.push_back({iter, 0, e2, evused - 1}); }
+        size_t e3 = evused;
+        if (prof) stage_event(ws, evpool, evused);
+        launch_center<D>(st, n, ws->Yn.p, ws->Y.p, ws->part.p, ws->sc.p, nullptr, nullptr);
+        ws->n_launch += 2;
+
+        if (p.enable_early_stopping && iter >= p.min_iter - 1) {
+            ws->Yconv.exact(ws->vbytes * n);
+            ws->convpart.exact(256);
+            const int vs = (int)(ws->vbytes / sizeof(float));
+            if (iter >= p.min_iter) {
+                k_conv_check<<<148, 256, 0, st>>>(n, (const float *)ws->Y.p, (const float *)ws->Yconv.p, ws->d, vs,
+                                                  ws->convpart.p);
+                double hm[148];
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(hm, ws->convpart.p, sizeof(hm), cudaMemcpyDeviceToHost, st));
+                TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+                double mx = 0.0;
+                for (double x : hm) mx = std::max(mx, x);
+                if (mx < p.convergence_tol) {
+                    ws->convergence_count++;
+                    if (ws->convergence_count >= p.convergence_patience) {
+                        ws->converged = 1;
+                        if (verbose) printf("\n*** CONVERGED at iteration %d ***\n", iter + 1);
+                        TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->Yconv.p, ws->Y.p, ws->vbytes * n, cudaMemcpyDeviceToDevice, st));
+                        break;
+                    }
+                } else {
+                    ws->convergence_count = 0;
+                }
+            }
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->Yconv.p, ws->Y.p, ws->vbytes * n, cudaMemcpyDeviceToDevice, st));
+        }
+        if (prof) { stage_event(ws, evpool, evused); stages.push_back({iter, 3, e3, evused - 1}); }
+
+        if (verbose && (iter % print_freq == 0 || iter == n_iter - 1 || iter % 50 == 0)) {
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+            TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+            if (iter % print_freq == 0 || iter == n_iter - 1)
+                printf("  Iteration %4d/%d: Z=%.3e, time=%.3f sec\n", iter + 1, n_iter,
+                       reuse ? ws->hsc.p->rep_Z : ws->hsc.p->Z, wall_sec() - t_iter);
+            if (iter % 50 == 0) printf("  [KL iter %4d] KL divergence: %.5f\n", iter, ws->hsc.p->kl);
+        }
+        if ((size_t)iter < ws->iter_times.size()) ws->iter_times[iter] = wall_sec() - t_iter;
+    }
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (it_end >= n_iter || ret != 0) ws->kl = ws->hsc.p->kl;
+    if (prof) {
+        for (const StageEv &s : stages) {
+            float ms = 0.f;
+            TSNE_CUDA_CHECK(cudaEventElapsedTime(&ms, evpool[s.a], evpool[s.b]));
+            const double sec = ms * 1e-3;
+            if (s.iter < 0 || s.iter >= n_iter) continue;
+            if (s.stage == 0) ws->prof->p_matvec_time[s.iter] += sec;
+            else if (s.stage == 1) ws->prof->h2_rebuild_time[s.iter] += sec;
+            else if (s.stage == 2) ws->prof->h2_matvec_s_time[s.iter] += sec;
+            else ws->prof->other_time[s.iter] += sec;
+        }
+        for (cudaEvent_t e : evpool) cudaEventDestroy(e);
+    }
+    (void)launch0;
+    return ret;
+}
+
+}  // namespace
+
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+tsne_params_t tsne_create_default_params(void)
+{
+    tsne_params_t p;
+    memset(&p, 0, sizeof(p));
+    p.n_iter = 1000;
+    p.perplexity = 30.0;
+    p.learning_rate = -1.0;
+    p.initial_momentum = 0.5;
+    p.momentum = 0.8;
+    p.momentum_switch_iter = 250;
+    p.early_exag = 12.0;
+    p.early_exag_iter = 250;
+    p.use_vptree = 2;
+    p.h2_tol = 1e-3;
+    p.h2_rebuild_freq = 10;
+    p.h2pack_print_level = 0;
+    p.init_method = 0;
+    p.init_Y = nullptr;
+    p.random_seed = (int)(unsigned int)time(nullptr);
+    p.verbose = 1;
+    p.print_freq = 50;
+    p.enable_early_stopping = 0;
+    p.convergence_tol = 1e-5;
+    p.convergence_patience = 10;
+    p.min_iter = 250;
+    p.sklearn_compatible = 1;
+    p.enable_profiling = 0;
+    p.profiling_output_file = nullptr;
+    p.num_threads = 1;
+    p.h2_leaf_size = 100;
+    p.h2_rebuild_freq_early = 10;
+    return p;
+}
+
+sparse_matrix_t *sparse_matrix_create(int n_rows, int n_cols, int nnz)
+{
+    if (n_rows < 0 || nnz < 0) return nullptr;
+    sparse_matrix_t *m = (sparse_matrix_t *)malloc(sizeof(sparse_matrix_t));
+    if (m == nullptr) return nullptr;
+    m->n_rows = n_rows;
+    m->n_cols = n_cols;
+    m->nnz = nnz;
+    m->row_ptr = (int *)malloc(sizeof(int) * ((size_t)n_rows + 1));
+    m->col_idx = (int *)malloc(sizeof(int) * ((size_t)nnz > 0 ? nnz : 1));
+    m->values = (double *)malloc(sizeof(double) * ((size_t)nnz > 0 ? nnz : 1));
+    if (!m->row_ptr || !m->col_idx || !m->values) { sparse_matrix_destroy(m); return nullptr; }
+    return m;
+}
+
+void sparse_matrix_destroy(sparse_matrix_t *mat)
+{
+    if (mat == nullptr) return;
+    free(mat->row_ptr);
+    free(mat->col_idx);
+    free(mat->values);
+    free(mat);
+}
+
+void sparse_matvec(const sparse_matrix_t *A, const double *x, double *y)
+{
+    for (int i = 0; i < A->n_rows; i++) {
+        double s = 0.0;
+        for (int e = A->row_ptr[i]; e < A->row_ptr[i + 1]; e++) s += A->values[e] * x[A->col_idx[e]];
+        y[i] = s;
+    }
+}
+
+void initialize_embedding(double *Y, int n_point, int low_dim, int method, const double *Y0, unsigned int seed)
+{
+    if (method == 1 && Y0 != nullptr) {
+        memcpy(Y, Y0, sizeof(double) * (size_t)n_point * low_dim);
+        return;
+    }
+    if (method == 1) printf("Warning: init_method=1 without init_Y, using random initialization\n");
+    // N(0, 1e-4^2) by Box-Muller on the C library's rand(), the reference's generator
+    srand(seed);
+    const long total = (long)n_point * low_dim;
+    for (long i = 0; i < total; i += 2) {
+        double u1 = (double)rand() / RAND_MAX;
+        double u2 = (double)rand() / RAND_MAX;
+        if (u1 < 1e-10) u1 = 1e-10;
+        const double rad = sqrt(-2.0 * log(u1));
+        Y[i] = 1e-4 * (rad * cos(2.0 * M_PI * u2));
+        if (i + 1 < total) Y[i + 1] = 1e-4 * (rad * sin(2.0 * M_PI * u2));
+    }
+}
+
+sparse_matrix_t *compute_P_from_knn_distances(const double *knn_distances, const int *knn_indices,
+                                              const int *knn_indptr, int n_samples, int nnz, double perplexity,
+                                              int num_threads)
+{
+    (void)num_threads;
+    if (n_samples < 0 || nnz < 0 || perplexity <= 0.0) return nullptr;
+    sparse_matrix_t *P = sparse_matrix_create(n_samples, n_samples, nnz);
+    if (P == nullptr) return nullptr;
+    memcpy(P->row_ptr, knn_indptr, sizeof(int) * ((size_t)n_samples + 1));
+    if (nnz > 0) memcpy(P->col_idx, knn_indices, sizeof(int) * nnz);
+    P->nnz = nnz;
+    P->row_ptr[n_samples] = nnz;
+    if (nnz == 0) return P;
+    try {
+        cudaStream_t st;
+        TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        DevBuf<int> ip;
+        DevBuf<double> dist, out;
+        ip.exact(n_samples + 1);
+        dist.exact(nnz);
+        out.exact(nnz);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(ip.p, knn_indptr, sizeof(int) * (n_samples + 1), cudaMemcpyHostToDevice, st));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(dist.p, knn_distances, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+        launch_pcal(st, n_samples, ip.p, dist.p, perplexity, out.p);
+        TSNE_CUDA_CHECK(cudaGetLastError());
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(P->values, out.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, st));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+        cudaStreamDestroy(st);
+    } catch (const CudaError &) {
+        sparse_matrix_destroy(P);
+        return nullptr;
+    }
+    return P;
+}
+
+tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int low_dim,
+                                   const tsne_params_t *params, sparse_matrix_t *P)
+{
+    (void)X;
+    if (low_dim != 2 && low_dim != 3) {
+        printf("Error: low_dim must be 2 or 3 (got %d)\n", low_dim);
+        return nullptr;
+    }
+    if (P == nullptr || P->n_rows != n_point || P->n_cols != n_point) {
+        printf("Error: Invalid P matrix (expected %dx%d, got %dx%d)\n", n_point, n_point, P ? P->n_rows : 0,
+               P ? P->n_cols : 0);
+        return nullptr;
+    }
+    if (params == nullptr || n_point < 1) return nullptr;
+    tsne_workspace *ws = new tsne_workspace();
+    try {
+        ws->params = *params;
+        if (params->profiling_output_file) ws->prof_file = params->profiling_output_file;
+        ws->params.profiling_output_file = nullptr;
+        ws->n = n_point;
+        ws->d = low_dim;
+        ws->pt_dim = pt_dim;
+        ws->lr = params->learning_rate < 0.0 ? std::max(200.0, n_point / 12.0) : params->learning_rate;
+        if (params->learning_rate < 0.0 && params->verbose)
+            printf("Using adaptive learning rate: %.1f (N=%d)\n", ws->lr, n_point);
+        ws->vbytes = low_dim == 2 ? vec_bytes<2>() : vec_bytes<3>();
+        ws->P = P;
+        TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&ws->st, cudaStreamNonBlocking));
+        const size_t vb = ws->vbytes * n_point;
+        ws->Y.exact(vb); ws->Yn.exact(vb); ws->uY.exact(vb); ws->gains.exact(vb); ws->rep.exact(vb);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(ws->uY.p, 0, vb, ws->st));
+        TSNE_CUDA_CHECK(cudaMemsetAsync(ws->rep.p, 0, vb, ws->st));
+        if (low_dim == 2) launch_fill_vec<2>(ws->st, n_point, ws->gains.p, 1.0f);
+        else launch_fill_vec<3>(ws->st, n_point, ws->gains.p, 1.0f);
+        ws->sc.exact(1);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(ws->sc.p, 0, sizeof(DevScalars), ws->st));
+        ws->part.exact((size_t)ROW_GRID * 3);
+        ws->zpart.exact(148 * 2 * 3);
+        ws->klpart.exact(ROW_GRID);
+        upload_P(ws);
+        std::vector<double> Y0((size_t)n_point * low_dim);
+        initialize_embedding(Y0.data(), n_point, low_dim, params->init_method, params->init_Y,
+                             (unsigned int)params->random_seed);
+        ws->params.init_Y = nullptr;
+        upload_soa(ws, Y0.data(), ws->Y.p);
+        ws->iter_times.assign(std::max(params->n_iter, 0), 0.0);
+        if (params->enable_profiling) {
+            const size_t ni = std::max(params->n_iter, 1);
+            ws->prof = (profiling_data_t *)calloc(1, sizeof(profiling_data_t));
+            ws->prof->knn_time = (double *)calloc(1, sizeof(double));
+            ws->prof->p_construction_time = (double *)calloc(1, sizeof(double));
+            ws->prof->p_matvec_time = (double *)calloc(ni, sizeof(double));
+            ws->prof->h2_rebuild_time = (double *)calloc(ni, sizeof(double));
+            ws->prof->h2_matvec_s_time = (double *)calloc(ni, sizeof(double));
+            ws->prof->h2_matvec_v_time = (double *)calloc(ni, sizeof(double));
+            ws->prof->z_computation_time = (double *)calloc(ni, sizeof(double));
+            ws->prof->gradient_time = (double *)calloc(ni, sizeof(double));
+            ws->prof->other_time = (double *)calloc(ni, sizeof(double));
+        }
+        if (params->verbose)
+            printf("Initializing t-SNE with pre-computed P matrix (n=%d, pt_dim=%d, low_dim=%d)\n", n_point, pt_dim,
+                   low_dim);
+        const bool never_h2 = (params->h2_rebuild_freq > 0 ? params->h2_rebuild_freq : 10) > 100000;
+        if (n_point >= 2000 && !never_h2) {
+            if (rebuild_h2(ws) != 0) {
+                printf("Error: Failed to build initial H2 matrix\n");
+                tsne_destroy(ws);
+                return nullptr;
+            }
+        }
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+    } catch (const CudaError &) {
+        tsne_destroy(ws);
+        return nullptr;
+    }
+    return ws;
+}
+
+int tsne_run_range(tsne_workspace_t *ws, int iter_begin, int iter_end)
+{
+    if (ws == nullptr) return -1;
+    try {
+        const long long l0 = ws->n_launch;
+        const int rc = ws->d == 2 ? run_range_impl<2>(ws, iter_begin, iter_end) : run_range_impl<3>(ws, iter_begin, iter_end);
+        (void)l0;
+        return rc;
+    } catch (const CudaError &) {
+        return -1;
+    }
+}
+
+int tsne_run(tsne_workspace_t *ws)
+{
+    if (ws == nullptr) return -1;
+    if (ws->params.verbose) printf("\nStarting t-SNE optimization (%d iterations)\n", ws->params.n_iter);
+    const long long l0 = ws->n_launch;
+    const int rc = tsne_run_range(ws, 0, ws->params.n_iter);
+    ws->n_launch = ws->n_launch - l0;
+    if (ws->params.verbose) printf("\nOptimization complete\n");
+    if (rc == 0 && ws->prof && !ws->prof_file.empty()) tsne_write_profiling_data(ws, ws->prof_file.c_str());
+    return rc;
+}
+
+void tsne_get_embedding(tsne_workspace_t *ws, double *Y_out)
+{
+    if (ws == nullptr || Y_out == nullptr) return;
+    try {
+        download_soa(ws, ws->Y.p, Y_out);
+    } catch (const CudaError &) {
+    }
+}
+
+double compute_kl_divergence(tsne_workspace_t *ws)
+{
+    if (ws == nullptr) return 0.0;
+    return ws->kl;
+}
+
+void tsne_destroy(tsne_workspace_t *ws)
+{
+    if (ws == nullptr) return;
+    if (ws->st) cudaStreamSynchronize(ws->st);
+    ws->h2.reset();
+    if (ws->P) sparse_matrix_destroy(ws->P);
+    if (ws->prof) {
+        free(ws->prof->knn_time); free(ws->prof->p_construction_time); free(ws->prof->p_matvec_time);
+        free(ws->prof->h2_rebuild_time); free(ws->prof->h2_matvec_s_time); free(ws->prof->h2_matvec_v_time);
+        free(ws->prof->z_computation_time); free(ws->prof->gradient_time); free(ws->prof->other_time);
+        free(ws->prof);
+    }
+    cudaStream_t st = ws->st;
+    delete ws;   // device buffers are released here
+    if (st) cudaStreamDestroy(st);
+}
+
+int tsne_fit_transform_with_P(const double *X, int n_point, int pt_dim, int low_dim, const tsne_params_t *params,
+                              sparse_matrix_t *P, double *Y_out)
+{
+    tsne_workspace_t *ws = tsne_init_with_P(X, n_point, pt_dim, low_dim, params, P);
+    if (ws == nullptr) return -1;
+    const int rc = tsne_run(ws);
+    if (rc != 0) { tsne_destroy(ws); return rc; }
+    tsne_get_embedding(ws, Y_out);
+    tsne_destroy(ws);
+    return 0;
+}
+
+void tsne_write_profiling_data(tsne_workspace_t *ws, const char *filename)
+{
+    if (ws == nullptr || ws->prof == nullptr || filename == nullptr) return;
+    FILE *fp = fopen(filename, "w");
+    if (!fp) { fprintf(stderr, "Error: Cannot write profiling data to %s\n", filename); return; }
+    profiling_data_t *pr = ws->prof;
+    const int n_iter = ws->params.n_iter;
+    fprintf(fp, "iteration,p_matvec,h2_rebuild,h2_matvec_s,h2_matvec_v,z_computation,gradient,other,total\n");
+    double tp = 0, tr = 0, tm = 0, tg = 0, tt = 0;
+    for (int i = 0; i < n_iter; i++) {
+        const double tot = pr->p_matvec_time[i] + pr->h2_rebuild_time[i] + pr->h2_matvec_s_time[i] +
+                           pr->h2_matvec_v_time[i] + pr->z_computation_time[i] + pr->gradient_time[i] + pr->other_time[i];
+        fprintf(fp, "%d,%.6f,%.6f,%.6f,%.6f,%.6f,%.6f,%.6f,%.6f\n", i, pr->p_matvec_time[i], pr->h2_rebuild_time[i],
+                pr->h2_matvec_s_time[i], pr->h2_matvec_v_time[i], pr->z_computation_time[i], pr->gradient_time[i],
+                pr->other_time[i], tot);
+        tp += pr->p_matvec_time[i];
+        tr += pr->h2_rebuild_time[i];
+        tm += pr->h2_matvec_s_time[i] + pr->h2_matvec_v_time[i];
+        tg += pr->gradient_time[i];
+        tt += tot;
+    }
+    const double tdiv = tt > 0 ? tt : 1.0;
+    fprintf(fp, "\n# Summary Statistics\n");
+    fprintf(fp, "# k-NN time: %.3f seconds\n", pr->knn_time[0]);
+    fprintf(fp, "# P construction: %.3f seconds\n", pr->p_construction_time[0]);
+    fprintf(fp, "# Total P-matvec: %.3f seconds (%.1f%%)\n", tp, 100.0 * tp / tdiv);
+    fprintf(fp, "# Total H²-rebuild: %.3f seconds (%.1f%%)\n", tr, 100.0 * tr / tdiv);
+    fprintf(fp, "# Total H²-matvec: %.3f seconds (%.1f%%)\n", tm, 100.0 * tm / tdiv);
+    fprintf(fp, "# Total gradient: %.3f seconds (%.1f%%)\n", tg, 100.0 * tg / tdiv);
+    fprintf(fp, "# Total optimization time: %.3f seconds\n", tt);
+    fclose(fp);
+    if (ws->params.verbose) printf("\nProfiling data written to: %s\n", filename);
+}
+
+void tsne_set_init_profiling_times(tsne_workspace_t *ws, double knn_time, double p_construction_time)
+{
+    if (ws == nullptr || ws->prof == nullptr) return;
+    ws->prof->knn_time[0] = knn_time;
+    ws->prof->p_construction_time[0] = p_construction_time;
+}
+
+void compute_attractive_forces(const sparse_matrix_t *P, const double *Y, int low_dim, int n_point,
+                               double early_exag, double *grad, int num_threads)
+{
+    (void)num_threads;
+    if (P == nullptr || Y == nullptr || grad == nullptr || (low_dim != 2 && low_dim != 3)) return;
+    sparse_matrix_t *Pc = sparse_matrix_create(P->n_rows, P->n_cols, P->row_ptr[P->n_rows]);
+    if (Pc == nullptr) return;
+    memcpy(Pc->row_ptr, P->row_ptr, sizeof(int) * (P->n_rows + 1));
+    memcpy(Pc->col_idx, P->col_idx, sizeof(int) * Pc->nnz);
+    memcpy(Pc->values, P->values, sizeof(double) * Pc->nnz);
+    tsne_workspace ws;
+    try {
+        ws.n = n_point; ws.d = low_dim; ws.P = Pc;
+        ws.vbytes = low_dim == 2 ? vec_bytes<2>() : vec_bytes<3>();
+        TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&ws.st, cudaStreamNonBlocking));
+        upload_P(&ws);
+        ws.Y.exact(ws.vbytes * n_point);
+        upload_soa(&ws, Y, ws.Y.p);
+        DevBuf<double> g;
+        g.exact((size_t)n_point * low_dim);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(g.p, grad, sizeof(double) * n_point * low_dim, cudaMemcpyHostToDevice, ws.st));
+        if (low_dim == 2) launch_attr_only<2>(ws.st, n_point, ws.rp.p, ws.col.p, ws.val.p, ws.Y.p, 4.0 * early_exag, g.p);
+        else launch_attr_only<3>(ws.st, n_point, ws.rp.p, ws.col.p, ws.val.p, ws.Y.p, 4.0 * early_exag, g.p);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(grad, g.p, sizeof(double) * n_point * low_dim, cudaMemcpyDeviceToHost, ws.st));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(ws.st));
+    } catch (const CudaError &) {
+    }
+    sparse_matrix_destroy(Pc);
+    ws.P = nullptr;
+    if (ws.st) cudaStreamDestroy(ws.st);
+    ws.st = nullptr;
+}
+
+H2Pack_p tsne_get_h2_matrix(tsne_workspace_t *ws)
+{
+    if (ws == nullptr || !ws->h2_valid) return nullptr;
+    static thread_local tsne_h2_matrix handle;
+    handle.ws = ws;
+    return &handle;
+}
+
+double compute_repulsive_forces_h2pack(H2Pack_p h2pack_W, const double *Y, int low_dim, int n_point,
+                                       tsne_workspace_t *ws, double *grad, int iter)
+{
+    (void)iter;
+    if (ws == nullptr || Y == nullptr || grad == nullptr || low_dim != ws->d || n_point != ws->n) return 1.0;
+    try {
+        std::vector<double> F((size_t)n_point * low_dim);
+        double Z = 1.0;
+        if (h2pack_W != nullptr && ws->h2_valid) {
+            // the H2 matrix applies to the embedding it was built from (the workspace's)
+            ws->h2->product_force(ws->frc.exact(ws->vbytes * n_point), ws->sc.p, ws->zpart.p, 0);
+        } else {
+            DevBuf<unsigned char> saveY;
+            saveY.exact(ws->vbytes * n_point);
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(saveY.p, ws->Y.p, ws->vbytes * n_point, cudaMemcpyDeviceToDevice, ws->st));
+            upload_soa(ws, Y, ws->Y.p);
+            if (ws->has_order) {
+                // Y is given in the caller's order; the workspace works in its own numbering
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->Y.p, saveY.p, ws->vbytes * n_point, cudaMemcpyDeviceToDevice, ws->st));
+                return 1.0;
+            }
+            if (low_dim == 2) exact_force<2>(ws); else exact_force<3>(ws);
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->Y.p, saveY.p, ws->vbytes * n_point, cudaMemcpyDeviceToDevice, ws->st));
+        }
+        download_soa(ws, ws->frc.p, F.data());
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, ws->st));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+        Z = ws->hsc.p->Z;
+        if (ws->hsc.p->force_ok)
+            for (size_t i = 0; i < F.size(); i++) grad[i] -= F[i];
+        return Z;
+    } catch (const CudaError &) {
+        return 1.0;
+    }
+}
+
+int update_h2_matrix(tsne_workspace_t *ws, int force_rebuild)
+{
+    (void)force_rebuild;
+    if (ws == nullptr) return -1;
+    try {
+        return rebuild_h2(ws);
+    } catch (const CudaError &) {
+        return -1;
+    }
+}
+
+int tsne_h2_matmul(H2Pack_p h2, const int nv, const double *const *X, double *const *Y, void **wsp)
+{
+    (void)wsp;
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2_valid || nv < 1 || nv > 4) return -1;
+    tsne_workspace *ws = h2->ws;
+    if (ws->has_order) return -1;
+    try {
+        const int n = ws->n;
+        std::vector<int> perm(n);
+        double corner[3], radius;
+        ws->h2->copy_tree(perm.data(), corner, &radius);
+        std::vector<float> xt((size_t)n * 4, 0.f), yt;
+        for (int k = 0; k < n; k++)
+            for (int c = 0; c < nv; c++) xt[(size_t)k * 4 + c] = (float)X[c][perm[k]];
+        ws->h2->product_columns(xt, yt);
+        for (int k = 0; k < n; k++)
+            for (int c = 0; c < nv; c++) Y[c][perm[k]] = (double)yt[(size_t)k * 4 + c] + X[c][perm[k]];
+        return 0;
+    } catch (const CudaError &) {
+        return -1;
+    }
+}
+
+void tsne_h2_matmul_free(void **wsp)
+{
+    if (wsp) *wsp = nullptr;
+}
+
+int tsne_renumber_points(tsne_workspace_t *ws, const int *ord, int num_threads)
+{
+    (void)num_threads;
+    if (ws == nullptr || ord == nullptr) return -1;
+    try {
+        DevBuf<int> d;
+        d.exact(ws->n);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(d.p, ord, sizeof(int) * ws->n, cudaMemcpyHostToDevice, ws->st));
+        renumber(ws, d.p);
+        ws->h2_valid = false;   // the tree refers to the old numbering
+        return 0;
+    } catch (const CudaError &) {
+        return -1;
+    }
+}
+
+int tsne_h2_info(H2Pack_p h2, int *n_node, int *max_level, int *n_far, int *n_near)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2) return -1;
+    const H2Stats &s = h2->ws->h2->stats();
+    if (n_node) *n_node = s.n_node;
+    if (max_level) *max_level = s.max_level;
+    if (n_far) *n_far = s.n_far;
+    if (n_near) *n_near = s.n_near;
+    return 0;
+}
+
+int tsne_h2_get_tree(H2Pack_p h2, int *perm, double *corner, double *radius)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2) return -1;
+    try { h2->ws->h2->copy_tree(perm, corner, radius); } catch (const CudaError &) { return -1; }
+    return 0;
+}
+
+int tsne_h2_get_nodes(H2Pack_p h2, int *start, int *end, int *level, int *parent, int *first_child, int *n_child,
+                      int *is_leaf)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2) return -1;
+    try { h2->ws->h2->copy_nodes(start, end, level, parent, first_child, n_child, is_leaf); } catch (const CudaError &) { return -1; }
+    return 0;
+}
+
+int tsne_h2_get_lists(H2Pack_p h2, int *far_ptr, int *far_idx, int *near_ptr, int *near_idx)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2) return -1;
+    try { h2->ws->h2->copy_lists(far_ptr, far_idx, near_ptr, near_idx); } catch (const CudaError &) { return -1; }
+    return 0;
+}
+
+int tsne_h2_get_ranks(H2Pack_p h2, int *rank)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2) return -1;
+    try { h2->ws->h2->copy_ranks(rank); } catch (const CudaError &) { return -1; }
+    return 0;
+}
+
+int tsne_get_state(tsne_workspace_t *ws, double *Y_out, double *rep_out, double *rep_Z)
+{
+    if (ws == nullptr) return -1;
+    try {
+        if (Y_out) download_soa(ws, ws->Y.p, Y_out);
+        if (rep_out) download_soa(ws, ws->rep.p, rep_out);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, ws->st));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+        if (rep_Z) *rep_Z = ws->hsc.p->rep_Z;
+    } catch (const CudaError &) {
+        return -1;
+    }
+    return 0;
+}
+
+int tsne_set_embedding(tsne_workspace_t *ws, const double *Y_in)
+{
+    if (ws == nullptr || Y_in == nullptr) return -1;
+    try {
+        std::vector<double> Yc((size_t)ws->n * ws->d);
+        if (ws->has_order) {
+            std::vector<int> ord(ws->n);
+            TSNE_CUDA_CHECK(cudaMemcpy(ord.data(), ws->order.p, sizeof(int) * ws->n, cudaMemcpyDeviceToHost));
+            for (int k = 0; k < ws->d; k++)
+                for (int j = 0; j < ws->n; j++) Yc[(size_t)k * ws->n + j] = Y_in[(size_t)k * ws->n + ord[j]];
+        } else {
+            memcpy(Yc.data(), Y_in, sizeof(double) * Yc.size());
+        }
+        upload_soa(ws, Yc.data(), ws->Y.p);
+        const size_t vb = ws->vbytes * ws->n;
+        TSNE_CUDA_CHECK(cudaMemsetAsync(ws->uY.p, 0, vb, ws->st));
+        if (ws->d == 2) launch_fill_vec<2>(ws->st, ws->n, ws->gains.p, 1.0f);
+        else launch_fill_vec<3>(ws->st, ws->n, ws->gains.p, 1.0f);
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+    } catch (const CudaError &) {
+        return -1;
+    }
+    return 0;
+}
+
+int tsne_get_run_stats(tsne_workspace_t *ws, int *n_rebuild, long long *n_launch)
+{
+    if (ws == nullptr) return -1;
+    if (n_rebuild) *n_rebuild = ws->n_rebuild;
+    if (n_launch) *n_launch = ws->n_launch;
+    return 0;
+}
+
+}  // extern "C"

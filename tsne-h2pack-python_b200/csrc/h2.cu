@@ -1,0 +1,1211 @@
+// Device H2 matrix of the t-SNE repulsive kernel K(x, y) = (1 + |x - y|^2)^-2.
+//
+// The reference builds and applies its H2 matrix through the H2Pack library
+// (src/tsne_h2pack.c:772-953 update_h2_matrix, src/tsne_h2_matmul.c:225-452 fused product),
+// which is absent from the reference checkout. This file is the engine's own design:
+//
+//   tree   : root box = bounding-box midpoint with half-width MIN_HALF_WIDTH * 2^k; 64-bit
+//            Morton keys of the points' cells at depth L; stable radix sort -> tree order;
+//            nodes split level by level (binary search of the child digit inside each node)
+//            while they hold more than leaf_size points. Nodes are numbered level by level
+//            in key order.
+//   lists  : per-target far / near partners of the symmetric dual-tree traversal, derived
+//            level by level from the parent's inadmissible-source set (NSET).
+//   bases  : for every node at level >= 2, an interpolative decomposition of K(candidates,
+//            proxy points): column-pivoted Gram-Schmidt in shared memory, one CTA per node,
+//            candidates = a leaf's points or the children's skeletons (nested bases).
+//   product: upward pass (warp per node), far field (warp per compressed target), near
+//            field (CTA per leaf, source tiles in shared memory), downward pass, then the Z
+//            identity and the force.
+// The CPU oracle (oracle/tsne_oracle.c) restates the same design; tree and lists agree bit
+// for bit.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "common.cuh"
+#include "devbuf.h"
+#include "h2.h"
+#include "kernels.h"
+
+namespace tsne {
+namespace {
+
+template <int D> using Vec = typename Dim<D>::vec;
+
+constexpr int ID_THREADS = 128;
+constexpr int NEAR_THREADS = 128;
+constexpr int STACK_CAP = 192;       // leaf-target descent stack (depth * (2^D - 1) + 2^D)
+
+struct TreeView {
+    int n, L, leaf_size, cap_node, nset_cap;
+    const unsigned long long *keys;
+    int *start, *end, *level, *parent, *fchild, *nchild, *leaf, *ix;
+    int *nch, *cb;
+    TreeInfo *info;
+};
+
+__device__ __forceinline__ int digit_of(unsigned long long key, int shift, int nchm1)
+{
+    return (int)((key >> shift) & (unsigned long long)nchm1);
+}
+
+// ---------------------------------------------------------------------------------
+// root box and keys
+// ---------------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_bbox(int n, const Vec<D> *__restrict__ Y, double *__restrict__ part)
+{
+    float lo[D], hi[D];
+    int bad = 0;
+    for (int k = 0; k < D; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> y = Y[i];
+        for (int k = 0; k < D; k++) {
+            const float v = vget(y, k);
+            if (!isfinite(v)) { bad++; continue; }
+            lo[k] = fminf(lo[k], v);
+            hi[k] = fmaxf(hi[k], v);
+        }
+    }
+    __shared__ float sl[256][D], sh[256][D];
+    __shared__ int sb[256];
+    for (int k = 0; k < D; k++) { sl[threadIdx.x][k] = lo[k]; sh[threadIdx.x][k] = hi[k]; }
+    sb[threadIdx.x] = bad;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            for (int k = 0; k < D; k++) {
+                sl[threadIdx.x][k] = fminf(sl[threadIdx.x][k], sl[threadIdx.x + s][k]);
+                sh[threadIdx.x][k] = fmaxf(sh[threadIdx.x][k], sh[threadIdx.x + s][k]);
+            }
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < D; k++) {
+            part[(size_t)blockIdx.x * (2 * D + 1) + k] = sl[0][k];
+            part[(size_t)blockIdx.x * (2 * D + 1) + D + k] = sh[0][k];
+        }
+        part[(size_t)blockIdx.x * (2 * D + 1) + 2 * D] = sb[0];
+    }
+}
+
+// Root box from the bounding box (min / max are exact in any order), then the root node.
+template <int D>
+__global__ void k_root(int n, int L, int nblk, const double *__restrict__ part, TreeView tv)
+{
+    if (threadIdx.x != 0) return;
+    double lo[D], hi[D], bad = 0.0;
+    for (int k = 0; k < D; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+    for (int b = 0; b < nblk; b++) {
+        for (int k = 0; k < D; k++) {
+            lo[k] = fmin(lo[k], part[(size_t)b * (2 * D + 1) + k]);
+            hi[k] = fmax(hi[k], part[(size_t)b * (2 * D + 1) + D + k]);
+        }
+        bad += part[(size_t)b * (2 * D + 1) + 2 * D];
+    }
+    TreeInfo *info = tv.info;
+    double ext = 0.0, ctr[D];
+    for (int k = 0; k < D; k++) {
+        ctr[k] = 0.5 * (lo[k] + hi[k]);
+        const double e = 0.5 * (hi[k] - lo[k]);
+        if (e > ext) ext = e;
+    }
+    double R = MIN_HALF_WIDTH;
+    for (int it = 0; it < 2100 && R < ext; it++) R *= 2.0;
+    info->nonfinite = bad > 0.0 ? 1 : 0;
+    info->radius = R;
+    for (int k = 0; k < 3; k++) info->corner[k] = k < D ? ctr[k] - R : 0.0;
+    info->n_node = 1;
+    info->max_level = 0;
+    info->max_leaf = 0;
+    info->nset_overflow = 0;
+    info->pad[0] = 0;   // node-capacity overflow
+    for (int l = 0; l < 32; l++) info->n_level_nodes[l] = 0;
+    for (int l = 0; l < 33; l++) info->level_begin[l] = 0;
+    info->n_level_nodes[0] = 1;
+    info->level_begin[1] = 1;
+    tv.start[0] = 0; tv.end[0] = n; tv.level[0] = 0; tv.parent[0] = -1;
+    tv.fchild[0] = -1; tv.nchild[0] = 0; tv.leaf[0] = 1;
+    tv.ix[0] = tv.ix[1] = tv.ix[2] = 0;
+}
+
+template <int D>
+__global__ void k_keys(int n, int L, const Vec<D> *__restrict__ Y, const TreeInfo *__restrict__ info,
+                       unsigned long long *__restrict__ keys, int *__restrict__ idx)
+{
+    const double R = info->radius;
+    const double cell = 2.0 * R / (double)(1LL << L);
+    const double qmax = (double)((1LL << L) - 1);
+    double corner[D];
+    for (int k = 0; k < D; k++) corner[k] = info->corner[k];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> y = Y[i];
+        unsigned int q[D];
+        for (int k = 0; k < D; k++) {
+            const double t = ((double)vget(y, k) - corner[k]) / cell;
+            double f;
+            if (!(t >= 0.0)) f = 0.0;
+            else if (t > qmax) f = qmax;
+            else f = floor(t);
+            q[k] = (unsigned int)f;
+        }
+        unsigned long long key = 0;
+        for (int b = L - 1; b >= 0; b--)
+            for (int k = D - 1; k >= 0; k--) key = (key << 1) | ((q[k] >> b) & 1u);
+        keys[i] = key;
+        idx[i] = i;
+    }
+}
+
+template <int D>
+__global__ void k_gather(int n, const int *__restrict__ perm, const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ xt)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) xt[i] = Y[perm[i]];
+}
+
+// ---------------------------------------------------------------------------------
+// tree levels: k_split finds the child ranges of the nodes of one level, k_emit (one
+// CTA) numbers the children in key order and writes them.
+// ---------------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_split(int l, TreeView tv)
+{
+    constexpr int NCH = 1 << D;
+    if (tv.info->pad[0]) return;   // node capacity exceeded: the host regrows and rebuilds
+    const int lb = tv.info->level_begin[l], nl = min(tv.info->n_level_nodes[l], tv.cap_node);
+    const int shift = D * (tv.L - l - 1);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
+        const int t = lb + j;
+        const int s = tv.start[t], e = tv.end[t];
+        int *cb = tv.cb + (size_t)j * (NCH + 1);
+        if (e - s <= tv.leaf_size || l >= tv.L) { tv.nch[j] = 0; continue; }
+        cb[0] = s;
+        cb[NCH] = e;
+        for (int c = 1; c < NCH; c++) {
+            int lo = s, hi = e;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (digit_of(tv.keys[mid], shift, NCH - 1) < c) lo = mid + 1; else hi = mid;
+            }
+            cb[c] = lo;
+        }
+        int cnt = 0;
+        for (int c = 0; c < NCH; c++) cnt += cb[c + 1] > cb[c];
+        tv.nch[j] = cnt;
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(1024) k_emit(int l, TreeView tv)
+{
+    constexpr int NCH = 1 << D;
+    using Scan = cub::BlockScan<int, 1024>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int s_run;
+    TreeInfo *info = tv.info;
+    if (info->pad[0]) return;
+    const int lb = info->level_begin[l], nl = min(info->n_level_nodes[l], tv.cap_node);
+    const int next = lb + nl;
+    if (threadIdx.x == 0) s_run = 0;
+    __syncthreads();
+    for (int chunk = 0; chunk < nl; chunk += 1024) {
+        const int j = chunk + threadIdx.x;
+        const int x = j < nl ? tv.nch[j] : 0;
+        int off, total;
+        Scan(tmp).ExclusiveSum(x, off, total);
+        const int run = s_run;
+        if (j < nl) {
+            const int t = lb + j;
+            int ml = 0;
+            if (x > 0) {
+                int child = next + run + off;
+                tv.fchild[t] = child;
+                tv.nchild[t] = x;
+                tv.leaf[t] = 0;
+                const int *cb = tv.cb + (size_t)j * (NCH + 1);
+                for (int c = 0; c < NCH; c++) {
+                    const int s = cb[c], e = cb[c + 1];
+                    if (e <= s) continue;
+                    if (child < tv.cap_node) {
+                        tv.start[child] = s; tv.end[child] = e; tv.level[child] = l + 1; tv.parent[child] = t;
+                        tv.fchild[child] = -1; tv.nchild[child] = 0; tv.leaf[child] = 1;
+                        for (int k = 0; k < 3; k++)
+                            tv.ix[(size_t)child * 3 + k] = k < D ? 2 * tv.ix[(size_t)t * 3 + k] + ((c >> k) & 1) : 0;
+                    } else {
+                        atomicExch(&info->pad[0], 1);
+                    }
+                    child++;
+                }
+            } else {
+                tv.fchild[t] = -1;
+                tv.nchild[t] = 0;
+                tv.leaf[t] = 1;
+                ml = tv.end[t] - tv.start[t];
+            }
+            if (ml > 0) atomicMax(&info->max_leaf, ml);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_run = run + total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int run = s_run;
+        info->level_begin[l + 1] = next;
+        if (l + 1 < 32) info->n_level_nodes[l + 1] = run;
+        info->level_begin[l + 2 < 33 ? l + 2 : 32] = next + run;
+        if (nl > 0) {
+            info->max_level = run > 0 ? l + 1 : l;
+            info->n_node = next + run;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// interaction lists
+// ---------------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ bool admissible(const TreeView &tv, int t, int s)
+{
+    const long long wt = 1LL << (tv.L - tv.level[t]);
+    const long long ws = 1LL << (tv.L - tv.level[s]);
+    long long dist = 0;
+    for (int k = 0; k < D; k++) {
+        const long long ct = 2LL * tv.ix[(size_t)t * 3 + k] * wt + wt;
+        const long long cs = 2LL * tv.ix[(size_t)s * 3 + k] * ws + ws;
+        const long long df = ct > cs ? ct - cs : cs - ct;
+        dist = df > dist ? df : dist;
+    }
+    return dist >= wt + ws + (long long)ADM_EXTRA * (wt < ws ? wt : ws);
+}
+
+struct ListOut {
+    int *far_cnt, *near_cnt;             // count pass
+    const int *far_ptr, *near_ptr;       // write pass
+    int *far_idx, *near_idx;
+    int *nset, *nset_cnt;
+    int write;
+};
+
+__device__ __forceinline__ void emit(int *idx, const int *ptr, int t, int &c, int v, int write)
+{
+    if (write) idx[ptr[t] + c] = v;
+    c++;
+}
+
+// leaf target t against the subtree of c (c neither admissible nor a leaf)
+template <int D>
+__device__ void descend(const TreeView &tv, ListOut &lo, int t, int c, int &fc, int &nc)
+{
+    int stk[STACK_CAP];
+    int sp = 0;
+    for (int k = tv.nchild[c] - 1; k >= 0; k--) stk[sp++] = tv.fchild[c] + k;
+    while (sp > 0) {
+        const int s = stk[--sp];
+        if (admissible<D>(tv, t, s)) { emit(lo.far_idx, lo.far_ptr, t, fc, s, lo.write); continue; }
+        if (tv.leaf[s]) { emit(lo.near_idx, lo.near_ptr, t, nc, s, lo.write); continue; }
+        if (sp + tv.nchild[s] > STACK_CAP) { atomicExch(&tv.info->nset_overflow, 1); return; }
+        for (int k = tv.nchild[s] - 1; k >= 0; k--) stk[sp++] = tv.fchild[s] + k;
+    }
+}
+
+template <int D>
+__device__ void process_target(const TreeView &tv, ListOut &lo, int t)
+{
+    int fc = 0, nc = 0, ns = 0;
+    if (t == 0) {
+        if (tv.leaf[0]) emit(lo.near_idx, lo.near_ptr, 0, nc, 0, lo.write);
+        else if (!lo.write) { lo.nset[0] = 0; ns = 1; }
+    } else {
+        const int p = tv.parent[t];
+        const int pn = lo.nset_cnt[p];
+        for (int a = 0; a < pn; a++) {
+            const int s = lo.nset[(size_t)p * tv.nset_cap + a];
+            const int c0 = tv.leaf[s] ? s : tv.fchild[s];
+            const int c1 = tv.leaf[s] ? s + 1 : tv.fchild[s] + tv.nchild[s];
+            for (int c = c0; c < c1; c++) {
+                if (c == t) {
+                    if (tv.leaf[t]) emit(lo.near_idx, lo.near_ptr, t, nc, t, lo.write);
+                    else if (!lo.write) {
+                        if (ns < tv.nset_cap) lo.nset[(size_t)t * tv.nset_cap + ns] = c;
+                        ns++;
+                    }
+                } else if (admissible<D>(tv, t, c)) {
+                    emit(lo.far_idx, lo.far_ptr, t, fc, c, lo.write);
+                } else if (tv.leaf[t]) {
+                    if (tv.leaf[c]) emit(lo.near_idx, lo.near_ptr, t, nc, c, lo.write);
+                    else descend<D>(tv, lo, t, c, fc, nc);
+                } else if (!lo.write) {
+                    if (ns < tv.nset_cap) lo.nset[(size_t)t * tv.nset_cap + ns] = c;
+                    ns++;
+                }
+            }
+        }
+    }
+    if (!lo.write) {
+        lo.far_cnt[t] = fc;
+        lo.near_cnt[t] = nc;
+        if (ns > tv.nset_cap) { atomicExch(&tv.info->nset_overflow, 1); ns = tv.nset_cap; }
+        lo.nset_cnt[t] = ns;
+    } else {
+        // ascending partners (insertion sort of this target's segments)
+        int *f = lo.far_idx + lo.far_ptr[t];
+        for (int a = 1; a < fc; a++) { const int v = f[a]; int z = a - 1; while (z >= 0 && f[z] > v) { f[z + 1] = f[z]; z--; } f[z + 1] = v; }
+        int *g = lo.near_idx + lo.near_ptr[t];
+        for (int a = 1; a < nc; a++) { const int v = g[a]; int z = a - 1; while (z >= 0 && g[z] > v) { g[z + 1] = g[z]; z--; } g[z + 1] = v; }
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_lists_level(int l, TreeView tv, ListOut lo)
+{
+    const int lb = tv.info->level_begin[l], nl = tv.info->n_level_nodes[l];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x)
+        process_target<D>(tv, lo, lb + j);
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_lists_write(int n_node, TreeView tv, ListOut lo)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x)
+        process_target<D>(tv, lo, t);
+}
+
+// rows of each node's interpolation matrix: a leaf's points, or (upper bound) the
+// children's skeletons; nodes above MIN_ADM_LEVEL are not compressed
+template <int D>
+__global__ void k_rowcap(int n_node, TreeView tv, int *__restrict__ rowcap)
+{
+    constexpr int NCH = 1 << D;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x) {
+        int r = 0;
+        if (tv.level[t] >= MIN_ADM_LEVEL) r = tv.leaf[t] ? tv.end[t] - tv.start[t] : NCH * Dim<D>::MAXR;
+        rowcap[t] = r;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) rowcap[n_node] = 0;
+}
+
+// ---------------------------------------------------------------------------------
+// proxy points (shells |y - c|_inf = rho h around a box of half-width h)
+// ---------------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ void proxy_point(int p, double h, float *out)
+{
+    if constexpr (D == 2) {
+        const int sh = p / SHELL_PTS_2D, k = p % SHELL_PTS_2D;
+        const double rad = shell_rho(sh) * h;
+        const double off = (sh & 1) ? 0.0 : 0.5;
+        const double u = ((double)k + off) * (8.0 / SHELL_PTS_2D);
+        const int side = (int)(u * 0.5);
+        const double a = u - 2.0 * side - 1.0;
+        double x, y;
+        switch (side) {
+            case 0: x = a; y = -1.0; break;
+            case 1: x = 1.0; y = a; break;
+            case 2: x = -a; y = 1.0; break;
+            default: x = -1.0; y = -a; break;
+        }
+        out[0] = (float)(x * rad);
+        out[1] = (float)(y * rad);
+    } else {
+        constexpr int g = SHELL_GRID_3D, per = 6 * g * g;
+        const int sh = p / per, r = p % per, f = r / (g * g), ij = r % (g * g), i = ij / g, j = ij % g;
+        const double rad = shell_rho(sh) * h;
+        const int ax = f >> 1;
+        const double sgn = (f & 1) ? 1.0 : -1.0;
+        const double a = ((double)i + 0.5) * (2.0 / g) - 1.0;
+        const double b = ((double)j + 0.5) * (2.0 / g) - 1.0;
+        double c[3];
+        c[ax] = sgn;
+        c[(ax + 1) % 3] = a;
+        c[(ax + 2) % 3] = b;
+        for (int k = 0; k < 3; k++) out[k] = (float)(c[k] * rad);
+    }
+}
+
+struct IdArgs {
+    TreeView tv;
+    const void *xt;
+    void *skel;
+    int *rank;
+    const long long *rowoff;
+    float *U;
+    float *gA, *gnrm;
+    int *gsel;
+    void *gcand;
+    int mcap;
+    float tol2;
+};
+
+template <int D>
+constexpr size_t id_smem_bytes(int mcap)
+{
+    constexpr int P = Dim<D>::NPROXY, MAXR = Dim<D>::MAXR;
+    return sizeof(float) * (size_t)P * D                 // proxies
+           + sizeof(float) * (size_t)MAXR * MAXR         // R11
+           + sizeof(Vec<D>) * (size_t)mcap               // candidates
+           + sizeof(float) * (size_t)mcap                // residual norms
+           + sizeof(int) * (size_t)mcap                  // pivot position per row
+           + sizeof(int) * (size_t)MAXR                  // pivot rows
+           + sizeof(float) * (size_t)P                   // current pivot direction
+           + sizeof(float) * (size_t)mcap * (P + 1);     // the matrix (row stride P + 1)
+}
+
+// Interpolative decomposition of one node (one CTA): A = K(candidates - c, proxies),
+// column-pivoted Gram-Schmidt over the rows of A until the largest residual row norm is
+// <= tol * the largest initial one; U = [I ; R11^-1 R12]^T in candidate order.
+template <int D>
+__global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
+{
+    constexpr int P = Dim<D>::NPROXY, PP = P + 1, MAXR = Dim<D>::MAXR;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const TreeView &tv = g.tv;
+    const int t = tv.info->level_begin[level] + blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const Vec<D> *xt = (const Vec<D> *)g.xt;
+    Vec<D> *skel = (Vec<D> *)g.skel;
+
+    unsigned char *ptr = smraw;
+    float *prox = (float *)ptr; ptr += sizeof(float) * P * D;
+    float *R11 = (float *)ptr; ptr += sizeof(float) * MAXR * MAXR;
+    Vec<D> *cand_s = (Vec<D> *)ptr; ptr += sizeof(Vec<D>) * g.mcap;
+    float *nrm_s = (float *)ptr; ptr += sizeof(float) * g.mcap;
+    int *selpos_s = (int *)ptr; ptr += sizeof(int) * g.mcap;
+    int *sel = (int *)ptr; ptr += sizeof(int) * MAXR;
+    float *q = (float *)ptr; ptr += sizeof(float) * P;
+    float *A_s = (float *)ptr;
+
+    __shared__ float s_bv[ID_THREADS / 32];
+    __shared__ int s_bi[ID_THREADS / 32];
+    __shared__ int s_best, s_stop;
+    __shared__ float s_n0;
+
+    const bool isleaf = tv.leaf[t] != 0;
+    int m = 0;
+    if (isleaf) m = tv.end[t] - tv.start[t];
+    else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
+    const long long roff = g.rowoff[t];
+    const bool glob = m > g.mcap;
+    float *A = glob ? g.gA + roff * PP : A_s;
+    float *nrm = glob ? g.gnrm + roff : nrm_s;
+    int *selpos = glob ? g.gsel + roff : selpos_s;
+    Vec<D> *cand = glob ? (Vec<D> *)g.gcand + roff : cand_s;
+    float *U = g.U + roff * MAXR;
+
+    const double h = tv.info->radius / (double)(1LL << level);
+    for (int p = tid; p < P; p += ID_THREADS) proxy_point<D>(p, h, prox + p * D);
+    float ctr[D];
+    for (int k = 0; k < D; k++)
+        ctr[k] = (float)(tv.info->corner[k] + (double)(2 * tv.ix[(size_t)t * 3 + k] + 1) * h);
+    if (isleaf) {
+        for (int a = tid; a < m; a += ID_THREADS) cand[a] = xt[tv.start[t] + a];
+    } else {
+        for (int a = tid; a < m; a += ID_THREADS) {
+            int c = tv.fchild[t], aa = a;
+            while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
+            cand[a] = skel[(size_t)c * MAXR + aa];
+        }
+    }
+    __syncthreads();
+
+    float lmax = 0.f;
+    for (int a = tid; a < m; a += ID_THREADS) {
+        const Vec<D> x = cand[a];
+        float rel[D];
+        for (int k = 0; k < D; k++) rel[k] = vget(x, k) - ctr[k];
+        float s2 = 0.f;
+        for (int p = 0; p < P; p++) {
+            float r2 = 0.f;
+            for (int k = 0; k < D; k++) { const float df = rel[k] - prox[p * D + k]; r2 = fmaf(df, df, r2); }
+            const float w = rkernel(r2);
+            A[(size_t)a * PP + p] = w;
+            s2 = fmaf(w, w, s2);
+        }
+        nrm[a] = s2;
+        selpos[a] = -1;
+        lmax = fmaxf(lmax, s2);
+    }
+    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if (lane == 0) s_bv[wid] = lmax;
+    __syncthreads();
+    if (tid == 0) {
+        float v = 0.f;
+        for (int w = 0; w < ID_THREADS / 32; w++) v = fmaxf(v, s_bv[w]);
+        s_n0 = v;
+    }
+    __syncthreads();
+    const float stop2 = g.tol2 * s_n0;
+    const int rmax = min(min(m, P), MAXR);
+    int r = 0;
+    while (r < rmax) {
+        float bv = -1.f;
+        int bi = INT_MAX;
+        for (int a = tid; a < m; a += ID_THREADS)
+            if (selpos[a] < 0 && (nrm[a] > bv)) { bv = nrm[a]; bi = a; }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0) { s_bv[wid] = bv; s_bi[wid] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            float v = s_bv[0];
+            int i = s_bi[0];
+            for (int w = 1; w < ID_THREADS / 32; w++)
+                if (s_bv[w] > v || (s_bv[w] == v && s_bi[w] < i)) { v = s_bv[w]; i = s_bi[w]; }
+            s_best = i;
+            s_stop = (i == INT_MAX) || !(v > stop2) || !(v > 0.f);
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const int best = s_best;
+        const float rr = sqrtf(nrm[best]);
+        const float inv = 1.0f / rr;
+        for (int p = tid; p < P; p += ID_THREADS) q[p] = A[(size_t)best * PP + p] * inv;
+        for (int k = tid; k < r; k += ID_THREADS) R11[k * MAXR + r] = U[(size_t)best * MAXR + k];
+        if (tid == 0) { R11[r * MAXR + r] = rr; selpos[best] = r; sel[r] = best; }
+        __syncthreads();
+        for (int a = tid; a < m; a += ID_THREADS) {
+            if (selpos[a] >= 0) continue;
+            float *row = A + (size_t)a * PP;
+            float dot = 0.f;
+            for (int p = 0; p < P; p++) dot = fmaf(q[p], row[p], dot);
+            float s2 = 0.f;
+            for (int p = 0; p < P; p++) { const float v = fmaf(-dot, q[p], row[p]); row[p] = v; s2 = fmaf(v, v, s2); }
+            nrm[a] = s2;
+            U[(size_t)a * MAXR + r] = dot;
+        }
+        __syncthreads();
+        r++;
+    }
+    for (int k = tid; k < r; k += ID_THREADS) skel[(size_t)t * MAXR + k] = cand[sel[k]];
+    if (tid == 0) g.rank[t] = r;
+    for (int a = tid; a < m; a += ID_THREADS) {
+        float *u = U + (size_t)a * MAXR;
+        const int pos = selpos[a];
+        if (pos >= 0) {
+            for (int k = 0; k < r; k++) u[k] = (k == pos) ? 1.f : 0.f;
+        } else {
+            for (int k = r - 1; k >= 0; k--) {
+                float acc = u[k];
+                for (int j = k + 1; j < r; j++) acc = fmaf(-R11[k * MAXR + j], u[j], acc);
+                u[k] = acc / R11[k * MAXR + k];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// product kernels
+// ---------------------------------------------------------------------------------
+struct ProdArgs {
+    TreeView tv;
+    const void *xt;
+    const void *skel;
+    const int *rank;
+    const long long *rowoff;
+    const float *U;
+    float4 *y0, *y1, *yp;
+    const int *far_ptr, *far_idx, *near_ptr, *near_idx;
+    const float4 *xin;   // input columns in tree order, or null for [1 | coordinates]
+};
+
+template <int D>
+__device__ __forceinline__ float4 input_at(const ProdArgs &g, const typename Dim<D>::vec *xt, int j);
+
+template <int D>
+__device__ __forceinline__ float4 with_one(const Vec<D> &x)
+{
+    if constexpr (D == 2) return make_float4(1.f, x.x, x.y, 0.f);
+    else return make_float4(1.f, x.x, x.y, x.z);
+}
+template <int D>
+__device__ __forceinline__ float4 input_at(const ProdArgs &g, const typename Dim<D>::vec *xt, int j)
+{
+    return g.xin ? g.xin[j] : with_one<D>(xt[j]);
+}
+__device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
+{
+    acc.x = fmaf(w, v.x, acc.x); acc.y = fmaf(w, v.y, acc.y);
+    acc.z = fmaf(w, v.z, acc.z); acc.w = fmaf(w, v.w, acc.w);
+}
+__device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
+
+// upward pass, one warp per node of `level`: y0[t] = U_t^T (leaf points | children's y0)
+template <int D>
+__global__ void __launch_bounds__(256) k_up(int level, ProdArgs g)
+{
+    constexpr int MAXR = Dim<D>::MAXR;
+    const TreeView &tv = g.tv;
+    const Vec<D> *xt = (const Vec<D> *)g.xt;
+    const int lb = tv.info->level_begin[level], nl = tv.info->n_level_nodes[level];
+    const int lane = threadIdx.x & 31;
+    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nl; j += (gridDim.x * blockDim.x) >> 5) {
+        const int t = lb + j;
+        const int r = g.rank[t];
+        const float *U = g.U + g.rowoff[t] * MAXR;
+        float4 acc[MAXR / 32];
+        for (int h = 0; h < MAXR / 32; h++) acc[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (tv.leaf[t]) {
+            const int m = tv.end[t] - tv.start[t];
+            for (int a = 0; a < m; a++) {
+                const float4 in = input_at<D>(g, xt, tv.start[t] + a);
+                for (int h = 0; h < MAXR / 32; h++) {
+                    const int k = lane + 32 * h;
+                    if (k < r) fma4(acc[h], U[(size_t)a * MAXR + k], in);
+                }
+            }
+        } else {
+            int a = 0;
+            for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) {
+                for (int kk = 0; kk < g.rank[c]; kk++, a++) {
+                    const float4 in = g.y0[(size_t)c * MAXR + kk];
+                    for (int h = 0; h < MAXR / 32; h++) {
+                        const int k = lane + 32 * h;
+                        if (k < r) fma4(acc[h], U[(size_t)a * MAXR + k], in);
+                    }
+                }
+            }
+        }
+        for (int h = 0; h < MAXR / 32; h++) {
+            const int k = lane + 32 * h;
+            if (k < r) g.y0[(size_t)t * MAXR + k] = acc[h];
+        }
+    }
+}
+
+// far field onto compressed targets, one warp per node at level >= 2:
+//   same-level partner  : y1[t] += K(J_t, J_s) y0[s]
+//   coarser leaf partner: y1[t] += K(J_t, X_s) [1 | x_s]
+template <int D>
+__global__ void __launch_bounds__(256) k_far_c(int first, int n_node, ProdArgs g)
+{
+    constexpr int MAXR = Dim<D>::MAXR;
+    const TreeView &tv = g.tv;
+    const Vec<D> *xt = (const Vec<D> *)g.xt;
+    const Vec<D> *skel = (const Vec<D> *)g.skel;
+    const int lane = threadIdx.x & 31;
+    for (int t = first + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t < n_node;
+         t += (gridDim.x * blockDim.x) >> 5) {
+        const int r = g.rank[t], lt = tv.level[t];
+        Vec<D> J[MAXR / 32];
+        float4 acc[MAXR / 32];
+        for (int h = 0; h < MAXR / 32; h++) {
+            const int k = lane + 32 * h;
+            J[h] = skel[(size_t)t * MAXR + (k < r ? k : 0)];
+            acc[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++) {
+            const int s = g.far_idx[e];
+            const int ls = tv.level[s];
+            if (ls == lt) {
+                const int rs = g.rank[s];
+                for (int b = 0; b < rs; b++) {
+                    const Vec<D> js = skel[(size_t)s * MAXR + b];
+                    const float4 y = g.y0[(size_t)s * MAXR + b];
+                    for (int h = 0; h < MAXR / 32; h++) fma4(acc[h], rkernel(dist2(J[h], js)), y);
+                }
+            } else if (ls < lt) {
+                for (int j = tv.start[s]; j < tv.end[s]; j++) {
+                    const Vec<D> x = xt[j];
+                    const float4 y = input_at<D>(g, xt, j);
+                    for (int h = 0; h < MAXR / 32; h++) fma4(acc[h], rkernel(dist2(J[h], x)), y);
+                }
+            }
+        }
+        for (int h = 0; h < MAXR / 32; h++) {
+            const int k = lane + 32 * h;
+            if (k < r) g.y1[(size_t)t * MAXR + k] = acc[h];
+        }
+    }
+}
+
+// near field onto a leaf's points (one CTA per leaf, sources tiled through shared memory):
+//   near partner           : yp[i] += sum_{j != i} K(x_i, x_j) [1 | x_j]
+//   finer far partner (s)  : yp[i] += K(x_i, J_s) y0[s]
+template <int D>
+__global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
+{
+    constexpr int MAXR = Dim<D>::MAXR;
+    const TreeView &tv = g.tv;
+    const int t = blockIdx.x;
+    if (!tv.leaf[t]) return;
+    const Vec<D> *xt = (const Vec<D> *)g.xt;
+    const Vec<D> *skel = (const Vec<D> *)g.skel;
+    __shared__ Vec<D> sx[NEAR_THREADS];
+    __shared__ float4 sxin[NEAR_THREADS];
+    __shared__ float4 sy[MAXR];
+    const int s0 = tv.start[t], cnt = tv.end[t] - s0, lt = tv.level[t];
+    for (int chunk = 0; chunk < cnt; chunk += NEAR_THREADS) {
+        const int i = s0 + chunk + threadIdx.x;
+        const bool valid = chunk + (int)threadIdx.x < cnt;
+        const Vec<D> xi = xt[valid ? i : s0];
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = g.near_ptr[t]; e < g.near_ptr[t + 1]; e++) {
+            const int s = g.near_idx[e];
+            const int ss = tv.start[s], sc = tv.end[s] - ss;
+            for (int tile = 0; tile < sc; tile += NEAR_THREADS) {
+                __syncthreads();
+                if ((int)threadIdx.x < sc - tile) {
+                    sx[threadIdx.x] = xt[ss + tile + threadIdx.x];
+                    sxin[threadIdx.x] = input_at<D>(g, xt, ss + tile + threadIdx.x);
+                }
+                __syncthreads();
+                const int lim = min(NEAR_THREADS, sc - tile);
+                for (int j = 0; j < lim; j++) {
+                    float w = rkernel(dist2(xi, sx[j]));
+                    w = (ss + tile + j == i) ? 0.f : w;
+                    fma4(acc, w, sxin[j]);
+                }
+            }
+        }
+        for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++) {
+            const int s = g.far_idx[e];
+            if (tv.level[s] <= lt) continue;
+            const int rs = g.rank[s];
+            __syncthreads();
+            for (int b = threadIdx.x; b < rs; b += NEAR_THREADS) {
+                sx[b] = skel[(size_t)s * MAXR + b];
+                sy[b] = g.y0[(size_t)s * MAXR + b];
+            }
+            __syncthreads();
+            for (int b = 0; b < rs; b++) fma4(acc, rkernel(dist2(xi, sx[b])), sy[b]);
+        }
+        if (valid) g.yp[i] = acc;
+    }
+}
+
+// downward pass, one warp per node of `level`: children's y1 / the leaf's points += U_t y1[t]
+template <int D>
+__global__ void __launch_bounds__(256) k_down(int level, ProdArgs g)
+{
+    constexpr int MAXR = Dim<D>::MAXR;
+    const TreeView &tv = g.tv;
+    const int lb = tv.info->level_begin[level], nl = tv.info->n_level_nodes[level];
+    const int lane = threadIdx.x & 31;
+    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nl; j += (gridDim.x * blockDim.x) >> 5) {
+        const int t = lb + j;
+        const int r = g.rank[t];
+        const float *U = g.U + g.rowoff[t] * MAXR;
+        float4 yr[MAXR / 32];
+        for (int h = 0; h < MAXR / 32; h++) {
+            const int k = lane + 32 * h;
+            yr[h] = k < r ? g.y1[(size_t)t * MAXR + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        const bool isleaf = tv.leaf[t] != 0;
+        int m = 0;
+        if (isleaf) m = tv.end[t] - tv.start[t];
+        else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
+        for (int a0 = 0; a0 < m; a0 += 32) {
+            const int a = a0 + lane;
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int k = 0; k < r; k++) {
+                const float4 y = make_float4(__shfl_sync(0xffffffffu, yr[k >> 5].x, k & 31),
+                                             __shfl_sync(0xffffffffu, yr[k >> 5].y, k & 31),
+                                             __shfl_sync(0xffffffffu, yr[k >> 5].z, k & 31),
+                                             __shfl_sync(0xffffffffu, yr[k >> 5].w, k & 31));
+                if (a < m) fma4(acc, U[(size_t)a * MAXR + k], y);
+            }
+            if (a < m) {
+                if (isleaf) {
+                    float4 o = g.yp[tv.start[t] + a];
+                    add4(o, acc);
+                    g.yp[tv.start[t] + a] = o;
+                } else {
+                    int c = tv.fchild[t], aa = a;
+                    while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
+                    float4 o = g.y1[(size_t)c * MAXR + aa];
+                    add4(o, acc);
+                    g.y1[(size_t)c * MAXR + aa] = o;
+                }
+            }
+        }
+    }
+}
+
+template <int D>
+__global__ void k_split_out(int n, const float4 *__restrict__ yp, float *__restrict__ s, Vec<D> *__restrict__ v)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = yp[i];
+        s[i] = a.x;
+        Vec<D> o;
+        if constexpr (D == 2) o = make_float2(a.y, a.z);
+        else o = make_float4(a.y, a.z, a.w, 0.f);
+        v[i] = o;
+    }
+}
+
+inline int grid_for(long long work, int block, int cap = 148 * 16)
+{
+    long long g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+// ---------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------
+template <int D>
+class H2Impl final : public H2Matrix {
+public:
+    H2Impl(int n, cudaStream_t st) : n_(n), st_(st)
+    {
+        keys_in_.exact(n); keys_.exact(n); idx_in_.exact(n); perm_.exact(n); xt_.exact(n);
+        yp_.exact(n); s_.exact(n); v_.exact(n);
+        bbox_part_.exact((size_t)BBOX_BLOCKS * (2 * D + 1));
+        info_.exact(1);
+        size_t b1 = 0, b2 = 0;
+        TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, b1, keys_in_.p, keys_.p, idx_in_.p,
+                                                        perm_.p, n, 0, D * Dim<D>::L, st_));
+        TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(nullptr, b2, (int *)nullptr, (int *)nullptr,
+                                                      n + 1, st_));
+        sort_bytes_ = b1;
+        cub_tmp_.exact(std::max(b1, b2) + 256);
+        cap_node_ = std::max(1024, 4 * (n / 16) + 1024);
+        alloc_nodes();
+        nset_cap_ = Dim<D>::NSET;
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)id_smem_bytes<D>(id_mcap())));
+    }
+
+    int build(const void *Y, int leaf_size, double tol) override
+    {
+        leaf_size_ = leaf_size;
+        const int L = Dim<D>::L;
+        for (int attempt = 0; attempt < 8; attempt++) {
+            k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
+            k_root<D><<<1, 32, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
+            k_keys<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, L, (const Vec<D> *)Y, info_.p, keys_in_.p, idx_in_.p);
+            size_t bytes = sort_bytes_;
+            TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, bytes, keys_in_.p, keys_.p, idx_in_.p,
+                                                            perm_.p, n_, 0, D * L, st_));
+            k_gather<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, perm_.p, (const Vec<D> *)Y, (Vec<D> *)xt_.p);
+            launches_ += 5 + 4;
+            int launched = 0;
+            int want = std::min(L + 1, std::max(6, last_max_level_ + 2));
+            bool overflow = false;
+            for (;;) {
+                for (int l = launched; l < want; l++) {
+                    k_split<D><<<grid_for(cap_node_, 256, 148 * 8), 256, 0, st_>>>(l, view());
+                    k_emit<D><<<1, 1024, 0, st_>>>(l, view());
+                    launches_ += 2;
+                }
+                launched = want;
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
+                TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+                const TreeInfo &I = *hinfo_.p;
+                if (I.nonfinite) return -1;
+                if (I.pad[0]) { overflow = true; break; }
+                if (launched <= L && launched < 31 && I.n_level_nodes[launched] > 0) {
+                    want = std::min(L + 1, launched + 4);
+                    continue;
+                }
+                break;
+            }
+            if (overflow) {
+                cap_node_ *= 2;
+                alloc_nodes();
+                continue;
+            }
+            break;
+        }
+        const TreeInfo &I = *hinfo_.p;
+        n_node_ = I.n_node;
+        max_level_ = I.max_level;
+        last_max_level_ = max_level_;
+        stats_.n_node = n_node_;
+        stats_.max_level = max_level_;
+        stats_.max_leaf = I.max_leaf;
+        if (max_level_ <= 2) { built_ = false; return 1; }
+
+        // interaction lists: count per level, scan, write
+        for (int attempt = 0; attempt < 4; attempt++) {
+            nset_.exact((size_t)n_node_ * nset_cap_);
+            nset_cnt_.exact(n_node_);
+            far_cnt_.exact(n_node_ + 1); near_cnt_.exact(n_node_ + 1);
+            far_ptr_.exact(n_node_ + 2); near_ptr_.exact(n_node_ + 2);
+            ListOut lo = list_out(0);
+            for (int l = 0; l <= max_level_; l++) {
+                k_lists_level<D><<<grid_for(I.n_level_nodes[l], 128, 148 * 8), 128, 0, st_>>>(l, view(), lo);
+                launches_++;
+            }
+            scan_exclusive(far_cnt_.p, far_ptr_.p, n_node_);
+            scan_exclusive(near_cnt_.p, near_ptr_.p, n_node_);
+            rowcap_.exact(n_node_ + 1);
+            rowoff_.exact(n_node_ + 2);
+            k_rowcap<D><<<grid_for(n_node_, 256), 256, 0, st_>>>(n_node_, view(), rowcap_.p);
+            scan_exclusive_ll(rowcap_.p, rowoff_.p, n_node_);
+            launches_ += 4;
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + n_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + n_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + n_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+            if (hinfo_.p->nset_overflow) { nset_cap_ *= 2; continue; }
+            break;
+        }
+        stats_.n_far = htot_[0];
+        stats_.n_near = htot_[1];
+        far_idx_.ensure(std::max(1, htot_[0]));
+        near_idx_.ensure(std::max(1, htot_[1]));
+        {
+            ListOut lo = list_out(1);
+            k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
+            launches_++;
+        }
+
+        // bases, bottom-up
+        constexpr int MAXR = Dim<D>::MAXR, P = Dim<D>::NPROXY;
+        rank_.exact(n_node_);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(rank_.p, 0, sizeof(int) * n_node_, st_));
+        skel_.ensure((size_t)n_node_ * MAXR);
+        y0_.ensure((size_t)n_node_ * MAXR);
+        y1_.ensure((size_t)n_node_ * MAXR);
+        U_.ensure((size_t)std::max<long long>(hrows_, 1) * MAXR);
+        const int mcap = id_mcap();
+        const bool need_glob = stats_.max_leaf > mcap || (1 << D) * MAXR > mcap;
+        if (need_glob) {
+            gA_.ensure((size_t)std::max<long long>(hrows_, 1) * (P + 1));
+            gnrm_.ensure(std::max<long long>(hrows_, 1));
+            gsel_.ensure(std::max<long long>(hrows_, 1));
+            gcand_.ensure(std::max<long long>(hrows_, 1));
+        }
+        IdArgs ia{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mcap,
+                  (float)((tol * ID_TOL_FACTOR) * (tol * ID_TOL_FACTOR))};
+        const size_t smem = id_smem_bytes<D>(mcap);
+        for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
+            const int nl = I.n_level_nodes[l];
+            if (nl > 0) { k_id<D><<<nl, ID_THREADS, smem, st_>>>(l, ia); launches_++; }
+        }
+        built_ = true;
+        rank_stats_valid_ = false;
+        return 0;
+    }
+
+    void product_force(void *F, DevScalars *sc, double *partials, int keep_rep) override
+    {
+        run_product();
+        k_split_out<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, yp_.p, s_.p, (Vec<D> *)v_.p);
+        launch_z_force<D>(st_, n_, xt_.p, s_.p, v_.p, perm_.p, F, sc, partials, 1, keep_rep);
+        launches_ += 3;
+    }
+
+    void product_host(std::vector<float> &s, std::vector<float> &v) override
+    {
+        run_product();
+        k_split_out<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, yp_.p, s_.p, (Vec<D> *)v_.p);
+        std::vector<float> st(n_);
+        std::vector<Vec<D>> vt(n_);
+        std::vector<int> perm(n_);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(st.data(), s_.p, sizeof(float) * n_, cudaMemcpyDeviceToHost, st_));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(vt.data(), v_.p, sizeof(Vec<D>) * n_, cudaMemcpyDeviceToHost, st_));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(perm.data(), perm_.p, sizeof(int) * n_, cudaMemcpyDeviceToHost, st_));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        s.assign(n_, 0.f);
+        v.assign((size_t)n_ * D, 0.f);
+        for (int k = 0; k < n_; k++) {
+            const int i = perm[k];
+            s[i] = st[k];
+            const float *vv = reinterpret_cast<const float *>(&vt[k]);
+            for (int c = 0; c < D; c++) v[(size_t)c * n_ + i] = vv[c];
+        }
+    }
+
+    void product_columns(const std::vector<float> &x_tree, std::vector<float> &y_tree) override
+    {
+        xin_.exact(n_);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(xin_.p, x_tree.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice, st_));
+        run_product(xin_.p);
+        y_tree.assign((size_t)n_ * 4, 0.f);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(y_tree.data(), yp_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, st_));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+    }
+
+    const int *perm_device() const override { return perm_.p; }
+
+    const H2Stats &stats() const override
+    {
+        if (!rank_stats_valid_ && built_) {
+            std::vector<int> r(n_node_);
+            cudaMemcpy(r.data(), rank_.p, sizeof(int) * n_node_, cudaMemcpyDeviceToHost);
+            int mx = 0; double sum = 0; int cnt = 0;
+            for (int x : r) if (x > 0) { mx = std::max(mx, x); sum += x; cnt++; }
+            stats_.rank_max = mx;
+            stats_.rank_mean = cnt ? sum / cnt : 0.0;
+            rank_stats_valid_ = true;
+        }
+        return stats_;
+    }
+
+    void copy_tree(int *perm, double *corner, double *radius) override
+    {
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        TSNE_CUDA_CHECK(cudaMemcpy(perm, perm_.p, sizeof(int) * n_, cudaMemcpyDeviceToHost));
+        TreeInfo I;
+        TSNE_CUDA_CHECK(cudaMemcpy(&I, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < D; k++) corner[k] = I.corner[k];
+        *radius = I.radius;
+    }
+
+    void copy_nodes(int *start, int *end, int *level, int *parent, int *fchild, int *nchild, int *leaf) override
+    {
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        const size_t b = sizeof(int) * n_node_;
+        TSNE_CUDA_CHECK(cudaMemcpy(start, start_.p, b, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(end, end_.p, b, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(level, level_.p, b, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(parent, parent_.p, b, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(fchild, fchild_.p, b, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(nchild, nchild_.p, b, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(leaf, leaf_.p, b, cudaMemcpyDeviceToHost));
+    }
+
+    void copy_lists(int *far_ptr, int *far_idx, int *near_ptr, int *near_idx) override
+    {
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        TSNE_CUDA_CHECK(cudaMemcpy(far_ptr, far_ptr_.p, sizeof(int) * (n_node_ + 1), cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(near_ptr, near_ptr_.p, sizeof(int) * (n_node_ + 1), cudaMemcpyDeviceToHost));
+        if (stats_.n_far) TSNE_CUDA_CHECK(cudaMemcpy(far_idx, far_idx_.p, sizeof(int) * stats_.n_far, cudaMemcpyDeviceToHost));
+        if (stats_.n_near) TSNE_CUDA_CHECK(cudaMemcpy(near_idx, near_idx_.p, sizeof(int) * stats_.n_near, cudaMemcpyDeviceToHost));
+    }
+
+    void copy_ranks(int *rank) override
+    {
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        if (built_) TSNE_CUDA_CHECK(cudaMemcpy(rank, rank_.p, sizeof(int) * n_node_, cudaMemcpyDeviceToHost));
+        else for (int i = 0; i < n_node_; i++) rank[i] = 0;
+    }
+
+    long long launches() const override { return launches_; }
+
+private:
+    static constexpr int BBOX_BLOCKS = 148 * 2;
+
+    static int id_mcap()
+    {
+        // shared-memory rows of the ID: every internal node of the 2D tree (4 * MAXR rows)
+        // and leaves up to that size; the 3D bound keeps the CTA under 227 KB
+        return D == 2 ? (1 << D) * Dim<D>::MAXR : 192;
+    }
+
+    void alloc_nodes()
+    {
+        const size_t c = cap_node_;
+        start_.exact(c); end_.exact(c); level_.exact(c); parent_.exact(c); fchild_.exact(c);
+        nchild_.exact(c); leaf_.exact(c); ix_.exact(3 * c); nch_.exact(c);
+        cb_.exact(c * ((1 << D) + 1));
+    }
+
+    TreeView view()
+    {
+        TreeView v;
+        v.n = n_; v.L = Dim<D>::L; v.leaf_size = leaf_size_; v.cap_node = cap_node_; v.nset_cap = nset_cap_;
+        v.keys = keys_.p; v.start = start_.p; v.end = end_.p; v.level = level_.p; v.parent = parent_.p;
+        v.fchild = fchild_.p; v.nchild = nchild_.p; v.leaf = leaf_.p; v.ix = ix_.p; v.nch = nch_.p;
+        v.cb = cb_.p; v.info = info_.p;
+        return v;
+    }
+
+    ListOut list_out(int write)
+    {
+        ListOut lo;
+        lo.far_cnt = far_cnt_.p; lo.near_cnt = near_cnt_.p;
+        lo.far_ptr = far_ptr_.p; lo.near_ptr = near_ptr_.p;
+        lo.far_idx = far_idx_.p; lo.near_idx = near_idx_.p;
+        lo.nset = nset_.p; lo.nset_cnt = nset_cnt_.p;
+        lo.write = write;
+        return lo;
+    }
+
+    // out[0] = 0, out[i + 1] = in[0] + ... + in[i]
+    void scan_exclusive(const int *in, int *out, int count)
+    {
+        TSNE_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(int), st_));
+        size_t need = 0;
+        TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(nullptr, need, in, out + 1, count, st_));
+        if (need > cub_tmp_.cap) cub_tmp_.exact(need + 256);
+        size_t bytes = cub_tmp_.cap;
+        TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(cub_tmp_.p, bytes, in, out + 1, count, st_));
+    }
+    void scan_exclusive_ll(const int *in, long long *out, int count)
+    {
+        TSNE_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(long long), st_));
+        size_t need = 0;
+        TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(nullptr, need, in, out + 1, count, st_));
+        if (need > cub_tmp_.cap) cub_tmp_.exact(need + 256);
+        size_t bytes = cub_tmp_.cap;
+        TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(cub_tmp_.p, bytes, in, out + 1, count, st_));
+    }
+
+    void run_product(const float4 *xin = nullptr)
+    {
+        ProdArgs g;
+        g.xin = xin;
+        g.tv = view(); g.xt = xt_.p; g.skel = skel_.p; g.rank = rank_.p; g.rowoff = rowoff_.p; g.U = U_.p;
+        g.y0 = y0_.p; g.y1 = y1_.p; g.yp = yp_.p;
+        g.far_ptr = far_ptr_.p; g.far_idx = far_idx_.p; g.near_ptr = near_ptr_.p; g.near_idx = near_idx_.p;
+        const TreeInfo &I = *hinfo_.p;
+        for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
+            const int nl = I.n_level_nodes[l];
+            if (nl > 0) { k_up<D><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
+        }
+        const int first = I.level_begin[MIN_ADM_LEVEL];
+        k_far_c<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(first, n_node_, g);
+        k_near<D><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
+        launches_ += 2;
+        for (int l = MIN_ADM_LEVEL; l <= max_level_; l++) {
+            const int nl = I.n_level_nodes[l];
+            if (nl > 0) { k_down<D><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
+        }
+    }
+
+    int n_;
+    cudaStream_t st_;
+    int leaf_size_ = 100;
+    int cap_node_ = 0, nset_cap_ = 0;
+    int n_node_ = 0, max_level_ = 0, last_max_level_ = 0;
+    bool built_ = false;
+    mutable bool rank_stats_valid_ = false;
+    mutable H2Stats stats_;
+    long long launches_ = 0;
+    size_t sort_bytes_ = 0;
+    int htot_[2] = {0, 0};
+    long long hrows_ = 0;
+
+    DevBuf<unsigned long long> keys_in_, keys_;
+    DevBuf<int> idx_in_, perm_;
+    DevBuf<Vec<D>> xt_;
+    DevBuf<unsigned char> cub_tmp_;
+    DevBuf<double> bbox_part_;
+    DevBuf<TreeInfo> info_;
+    HostPinned<TreeInfo> hinfo_;
+    DevBuf<int> start_, end_, level_, parent_, fchild_, nchild_, leaf_, ix_, nch_, cb_;
+    DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;
+    DevBuf<int> rowcap_;
+    DevBuf<long long> rowoff_;
+    DevBuf<int> rank_;
+    DevBuf<Vec<D>> skel_;
+    DevBuf<float4> y0_, y1_, yp_, xin_;
+    DevBuf<float> U_, s_;
+    DevBuf<Vec<D>> v_;
+    DevBuf<float> gA_, gnrm_;
+    DevBuf<int> gsel_;
+    DevBuf<Vec<D>> gcand_;
+};
+
+}  // namespace
+
+std::unique_ptr<H2Matrix> make_h2_matrix(int d, int n, cudaStream_t st)
+{
+    if (d == 2) return std::unique_ptr<H2Matrix>(new H2Impl<2>(n, st));
+    return std::unique_ptr<H2Matrix>(new H2Impl<3>(n, st));
+}
+
+}  // namespace tsne

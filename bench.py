@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the t-SNE optimisation phase (the reference's "Total optimization time").
+
+Workload: 1,000,000 x 50 float32 Gaussian mixture (100 clusters, Zipf(1.1) sizes, centres
+~N(0, 3^2 I), per-dimension std ~U(0.5, 2)), seed 1; exact k = 90 neighbour graph built once
+outside timing; perplexity 30; 2D; 1000 iterations (250 at exaggeration 12); h2_tol 1e-2,
+rebuild every 3 iterations (10 during early exaggeration), 100 points per leaf;
+init='random'. A step is one whole optimisation phase (tsne_run) on that input.
+
+  value   device time of tsne_run (CUDA events on the engine's stream), seconds, max over ranks
+  e2e     the same phase through the C ABI with host buffers: sparse_matrix_create + copy of P,
+          tsne_init_with_P (upload of P and Y0, first H2 build), tsne_run, tsne_get_embedding,
+          compute_kl_divergence, tsne_destroy
+  roofline  the attractive pass fused with the update (the kernel launched every iteration)
+  cpu_baseline  the CPU oracle (C/OpenMP port of the path) on a bounded sample, all host cores
+
+--impl reference times the reference path on the host cores instead (the oracle port: the
+reference's own H2 path cannot be built, its H2Pack dependency being absent).
+Multi-GPU (torchrun): every rank runs its own replica of the workload (no collective on the
+data path); value is the slowest rank's time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "tsne-h2pack-python_b200"))
+
+METRIC = "opt-phase s at 1M pts 2D"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "attr_update_traffic.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--iters", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--save-embedding", default=None)
+    return ap.parse_args()
+
+
+def workload(n, seed=1, device=0):
+    """X, graph G (CSR distances) and joint P of the benchmark input (setup, untimed)."""
+    from tsne_h2pack._synthetic import knn_graph_torch, mixture_zipf
+    from tsne_h2pack._backend import get_backend
+    X, _ = mixture_zipf(n, seed=seed)
+    G = knn_graph_torch(X, 90, device=f"cuda:{device}", chunk=4096 if n > 200_000 else 8192)
+    P = get_backend().joint_P(G, 30.0)
+    return X, G, P
+
+
+def params_for(be, n, iters):
+    p = be.create_default_params()
+    p.n_iter = iters
+    p.verbose = 0
+    p.perplexity = 30.0
+    p.learning_rate = max(n / 12.0, 200.0)
+    p.h2_tol, p.h2_rebuild_freq, p.h2_rebuild_freq_early, p.h2_leaf_size = 1e-2, 3, 10, 100
+    p.random_seed = 1
+    p.init_method = 0
+    return p
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        self.proc = None
+
+    def start(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1])); mx = max(mx, float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ours(args, rank, world, local):
+    import torch
+    from tsne_h2pack._backend import TSNEWorkspace, get_backend, scipy_csr_to_c_sparse_matrix
+    torch.cuda.set_device(local)
+    os.environ["TSNE_KERNEL_TIMING"] = "1"
+    be = get_backend()
+    lib = be._lib
+    lib.tsne_get_timing.argtypes = [ctypes.POINTER(TSNEWorkspace), ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    n = args.n
+    t0 = time.time()
+    X, G, P = workload(n, device=local)
+    setup_s = time.time() - t0
+    nnz = P.nnz
+    Yout = np.zeros((2, n))
+
+    def step():
+        """One e2e step through the C ABI; returns (wall s, device run s, attr ms, attr launches, launches)."""
+        prm = params_for(be, n, args.iters)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        Pc = scipy_csr_to_c_sparse_matrix(P, lib)
+        ws = lib.tsne_init_with_P(None, n, 0, 2, ctypes.byref(prm), Pc)
+        if not ws:
+            raise RuntimeError("tsne_init_with_P returned NULL")
+        rc = lib.tsne_run(ws)
+        if rc != 0:
+            raise RuntimeError(f"tsne_run failed ({rc})")
+        lib.tsne_get_embedding(ws, Yout)
+        kl = float(lib.compute_kl_divergence(ws))
+        run_ms, attr_ms, attr_n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        lib.tsne_get_timing(ws, ctypes.byref(run_ms), ctypes.byref(attr_ms), ctypes.byref(attr_n))
+        nr, nl = ctypes.c_int(), ctypes.c_longlong()
+        lib.tsne_get_run_stats(ws, ctypes.byref(nr), ctypes.byref(nl))
+        lib.tsne_destroy(ws)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        return wall, run_ms.value / 1e3, attr_ms.value, attr_n.value, nl.value, nr.value, kl
+
+    for _ in range(args.warmup):
+        step()
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    res = [step() for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    if dist:
+        tdist.barrier()
+    dev_s = float(np.mean([r[1] for r in res]))
+    wall_s = float(np.mean([r[0] for r in res]))
+    if dist:
+        t = torch.tensor([dev_s, wall_s], device=f"cuda:{local}", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        dev_s, wall_s = t.tolist()
+    attr_ms = sum(r[2] for r in res) / max(1, sum(r[3] for r in res))
+    launches = int(sum(r[4] for r in res))
+    kl = res[-1][6]
+    if args.save_embedding and rank == 0:
+        np.save(args.save_embedding, Yout)
+
+    out = None
+    if rank == 0:
+        peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
+        peak = peaks.get("hbm_gbs", 6650.0)
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        attr_bytes = 8.0 * (nnz) + 4.0 * (n + 1) + 28.0 * 2 * n
+        achieved = attr_bytes / (attr_ms * 1e-3) / 1e9
+        traffic = None
+        if TRAFFIC.exists():
+            tr = json.loads(TRAFFIC.read_text())
+            if tr.get("n") and tr.get("bytes_per_launch"):
+                traffic = tr["bytes_per_launch"] * (n / tr["n"])
+        h2d = 4 * (n + 1) + 12 * nnz + 16 * n
+        d2h = 16 * n + 8
+        out = {
+            "metric": METRIC, "value": round(dev_s, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dev_s * 1e3, 2), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: 1,000,000 x 50 float32 Zipf(1.1) Gaussian mixture, seed 1; exact k=90 graph",
+            "config": {"workload": f"{n:,} points x 50 dims -> 2D, {args.iters} iterations, perplexity 30, "
+                                   "h2_tol 1e-2, H2 rebuild every 3 (10 early), leaf 100, init random",
+                       "n_points": n, "nnz_P": int(nnz), "iterations": args.iters,
+                       "l2": "inputs larger than L2 (P streams 1.2 GB per iteration)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "k_attr_update (attractive CSR pass + gains/momentum update)",
+                         "avg_launch_ms": round(attr_ms, 4), "algorithmic_bytes": attr_bytes,
+                         "peak_source": peak_src},
+            "e2e": {"value": round(wall_s, 4), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches,
+            "kl_divergence": round(kl, 5),
+            "n_rebuild": res[-1][5],
+            "setup_s": round(setup_s, 1),
+        }
+        if ck:
+            out["clocks"] = ck
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_sample(P, n, args.iters)
+    return out
+
+
+def cpu_sample(P, n, iters):
+    """Bounded CPU sample of the same workload on the oracle port (all host cores):
+    iterations 0 and 1 (each an H2 build + product + attractive/update pass) and one more
+    attractive pass; the phase estimate uses the schedule's counts (rebuilds, passes)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    Y0 = O.init_embedding(n, 2, 1)
+    r = O.Runner(P, Y0, nthreads=cores, n_iter=iters)
+    t0 = time.perf_counter(); r.run(0, 1); t1 = time.perf_counter(); r.run(1, 2); t2 = time.perf_counter()
+    r.close()
+    ta = time.perf_counter(); O.attractive(P, Y0, 12.0, nthreads=cores); tb = time.perf_counter()
+    t_pass = tb - ta
+    t_rb = max(0.0, 0.5 * ((t1 - t0) + (t2 - t1)) - t_pass)
+    n_rb = rebuild_count(iters)
+    est = n_rb * t_rb + iters * t_pass
+    return {"value": round(est, 2), "unit": "s", "cores": cores, "kind": "port",
+            "sample": f"oracle (C/OpenMP FP64 port) iterations 0-1 of the {n:,}-point workload plus one attractive "
+                      f"pass ({t2 - t0 + t_pass:.1f} s); estimate = {n_rb} x (H2 build + product "
+                      f"{t_rb:.2f} s) + {iters} x pass {t_pass:.3f} s"}
+
+
+def rebuild_count(iters, freq=3, early=10, exag_iter=250):
+    c = 1
+    for it in range(1, iters):
+        eff = 1 if it < 20 else freq
+        if 20 <= it < exag_iter:
+            eff = max(eff, early)
+        c += it % eff == 0
+    return c
+
+
+def reference(args, rank, world, local):
+    if rank != 0:
+        return None
+    n = args.n
+    X, G, P = workload(n, device=local)
+    samples = [cpu_sample(P, n, args.iters) for _ in range(args.warmup + args.steps)][args.warmup:]
+    v = float(np.mean([s["value"] for s in samples]))
+    cb = dict(samples[-1])
+    cb["value"] = round(v, 2)
+    return {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v * 1e3, 1), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: 1,000,000 x 50 float32 Zipf(1.1) Gaussian mixture, seed 1; exact k=90 graph",
+            "config": {"workload": f"{n:,} points x 50 dims -> 2D, {args.iters} iterations, perplexity 30, "
+                                   "h2_tol 1e-2, H2 rebuild every 3 (10 early), leaf 100, init random",
+                       "n_points": n, "iterations": args.iters, "parallelism": "host cores"},
+            "cpu_baseline": cb, "e2e": {"value": round(v, 2), "unit": "s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        out = ours(args, rank, world, local) if args.impl == "ours" else reference(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

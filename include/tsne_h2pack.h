@@ -201,6 +201,10 @@ TSNE_API int tsne_get_state(tsne_workspace_t *workspace, DTYPE *Y_out, DTYPE *re
 TSNE_API int tsne_set_embedding(tsne_workspace_t *workspace, const DTYPE *Y_in);
 /* Run iterations [iter_begin, iter_end) of the schedule (tsne_run = [0, n_iter)) */
 TSNE_API int tsne_run_range(tsne_workspace_t *workspace, int iter_begin, int iter_end);
+/* Device time of the last tsne_run / tsne_run_range (CUDA events on the workspace's stream,
+ * ms) and, when the environment sets TSNE_KERNEL_TIMING=1, the summed device time and count of
+ * its attractive-pass launches */
+TSNE_API int tsne_get_timing(tsne_workspace_t *workspace, double *run_ms, double *attr_ms, int *attr_launches);
 /* Number of H2 rebuilds and kernel launches issued by the last tsne_run / tsne_run_range */
 TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, long long *n_launch);
 

@@ -383,3 +383,38 @@ def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=
     finally:
         L.tsne_destroy(ws)
     return Y, kl_val
+
+
+class Runner:
+    """A persistent oracle state for timing bounded samples of the optimisation phase."""
+
+    def __init__(self, P, Y0, nthreads=None, **kw):
+        Y0 = np.ascontiguousarray(Y0, dtype=np.float64)
+        self.d, self.n = Y0.shape
+        self._arrays = (np.ascontiguousarray(P.indptr, dtype=np.int32),
+                        np.ascontiguousarray(P.indices, dtype=np.int32),
+                        np.ascontiguousarray(P.data, dtype=np.float64))
+        rp, ci, pv = self._arrays
+        self.st = lib().ora_state_create(self.n, self.d, _p(rp, _i32p), _p(ci, _i32p), _p(pv, _f64p),
+                                         _p(Y0, _f64p))
+        n = self.n
+        self.prm = RunParams(n_iter=kw.get("n_iter", 1000), learning_rate=kw.get("learning_rate") or max(n / 12.0, 200.0),
+                             momentum=0.8, initial_momentum=0.5, momentum_switch_iter=250,
+                             early_exag=12.0, early_exag_iter=250, h2_tol=kw.get("h2_tol", 1e-2),
+                             h2_rebuild_freq=kw.get("h2_rebuild_freq", 3),
+                             h2_rebuild_freq_early=kw.get("h2_rebuild_freq_early", 10),
+                             h2_leaf_size=kw.get("h2_leaf_size", 100), use_h2=1, rep_reuse=1, reorder=1,
+                             nthreads=nthreads or nthreads_default(), iter_begin=0, iter_end=0)
+
+    def run(self, begin, end):
+        self.prm.iter_begin, self.prm.iter_end = begin, end
+        if lib().ora_run(self.st, ctypes.byref(self.prm)) != 0:
+            raise RuntimeError("ora_run failed")
+
+    def close(self):
+        if self.st:
+            lib().ora_state_free(self.st)
+            self.st = None
+
+    def __del__(self):
+        self.close()

@@ -110,6 +110,9 @@ struct tsne_workspace {
     int convergence_count = 0, converged = 0;
     std::vector<double> iter_times;
     profiling_data_t *prof = nullptr;
+    // device timing of the last run (CUDA events on the workspace stream)
+    double last_run_ms = 0.0, attr_ms = 0.0;
+    int attr_launches = 0;
 };
 
 struct tsne_h2_matrix {
@@ -330,6 +333,13 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
 
     // profiling: events per stage, resolved at the end
     const bool prof = ws->prof != nullptr;
+    const bool ktime = env_int("TSNE_KERNEL_TIMING", 0) != 0;
+    std::vector<cudaEvent_t> kev;
+    size_t kused = 0;
+    cudaEvent_t run0, run1;
+    TSNE_CUDA_CHECK(cudaEventCreate(&run0));
+    TSNE_CUDA_CHECK(cudaEventCreate(&run1));
+    TSNE_CUDA_CHECK(cudaEventRecord(run0, st));
     std::vector<cudaEvent_t> evpool;
     size_t evused = 0;
     struct StageEv { int iter; int stage; size_t a, b; };
@@ -410,8 +420,10 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
 
         size_t e2 = evused;
         if (prof) stage_event(ws, evpool, evused);
+        if (ktime) stage_event(ws, kev, kused);
         launch_attr_update<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p, ws->uY.p, ws->gains.p,
                               force, flag, (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
+        if (ktime) stage_event(ws, kev, kused);
         if (prof) { stage_event(ws, evpool, evused); stages.push_back({iter, 0, e2, evused - 1}); }
         size_t e3 = evused;
         if (prof) stage_event(ws, evpool, evused);
@@ -456,9 +468,25 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
         }
         if ((size_t)iter < ws->iter_times.size()) ws->iter_times[iter] = wall_sec() - t_iter;
     }
+    TSNE_CUDA_CHECK(cudaEventRecord(run1, st));
     TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     if (it_end >= n_iter || ret != 0) ws->kl = ws->hsc.p->kl;
+    {
+        float ms = 0.f;
+        TSNE_CUDA_CHECK(cudaEventElapsedTime(&ms, run0, run1));
+        ws->last_run_ms = ms;
+        cudaEventDestroy(run0);
+        cudaEventDestroy(run1);
+        ws->attr_ms = 0.0;
+        ws->attr_launches = 0;
+        for (size_t k = 0; k + 1 < kused; k += 2) {
+            TSNE_CUDA_CHECK(cudaEventElapsedTime(&ms, kev[k], kev[k + 1]));
+            ws->attr_ms += ms;
+            ws->attr_launches++;
+        }
+        for (cudaEvent_t e : kev) cudaEventDestroy(e);
+    }
     if (prof) {
         for (const StageEv &s : stages) {
             float ms = 0.f;
@@ -1003,6 +1031,15 @@ int tsne_set_embedding(tsne_workspace_t *ws, const double *Y_in)
     } catch (const CudaError &) {
         return -1;
     }
+    return 0;
+}
+
+int tsne_get_timing(tsne_workspace_t *ws, double *run_ms, double *attr_ms, int *attr_launches)
+{
+    if (ws == nullptr) return -1;
+    if (run_ms) *run_ms = ws->last_run_ms;
+    if (attr_ms) *attr_ms = ws->attr_ms;
+    if (attr_launches) *attr_launches = ws->attr_launches;
     return 0;
 }
 

@@ -3,7 +3,8 @@
 Tolerances (FP32 device state against FP64 oracles; t-SNE amplifies a rounding difference
 by roughly 2x per iteration, so trajectory comparisons stop after a few tens of
 iterations):
-  - exact path, 20 iterations, vs the reference's own build: max rel 2e-3
+  - exact path vs the reference's own build: max rel 1e-5 after 1 iteration, 1e-4 after 5;
+    KL within 0.1% after 10 iterations and 1% after 20
   - perplexity calibration vs the oracle: rtol 1e-10
   - H2 tree permutation, node table and near/far lists vs the oracle: bit-exact
   - H2 repulsive force vs the FP64 exact force: rel 2-norm <= h2_tol
@@ -36,7 +37,7 @@ def test_exact_path_matches_reference(small):
     """N < 2000 runs the exact O(N^2) repulsion every iteration, as the reference does. The
     device state is FP32: its rounding grows ~2x per iteration like any t-SNE perturbation
     (the FP64 oracle and the reference's own build drift apart the same way), so the
-    embeddings are compared after 5 iterations and the KL after 20."""
+    embeddings are compared after 5 iterations and the KL after 10 and 20."""
     X, G, P, _ = small
     Y0 = O.init_embedding(P.shape[0], 2, 11)
     ref = (lambda it: O.ref_run(P, Y0, it, learning_rate=200.0)) if O.ref_available() else \
@@ -46,10 +47,11 @@ def test_exact_path_matches_reference(small):
         eng.run_all()
         assert rel(eng.embedding(), ref(n_iter)[0]) < tol, n_iter
         eng.close()
-    eng = Engine(P, Y0, n_iter=20, learning_rate=200.0)
-    eng.run_all()
-    Yr, klr = ref(20)
-    assert abs(eng.kl() - klr) < 1e-3 * abs(klr)
+    for n_iter, tol in ((10, 1e-3), (20, 1e-2)):
+        eng = Engine(P, Y0, n_iter=n_iter, learning_rate=200.0)
+        eng.run_all()
+        Yr, klr = ref(n_iter)
+        assert abs(eng.kl() - klr) < tol * abs(klr), n_iter
 
 
 def test_exact_method_matches_oracle(mid):

@@ -418,6 +418,52 @@ __global__ void k_row_copy(int n, const int *__restrict__ ord, const int *__rest
     }
 }
 
+// Sort every row of a padded CSR by column (the renumbered P, reference tsne_reorder.c
+// leaves each row sorted by its new column numbers): one warp per row, bitonic sort of the
+// row in shared memory (rows up to SORT_ROW_MAX entries); longer rows are listed for the
+// caller, which sorts them separately.
+constexpr int SORT_ROW_MAX = 1024;
+__global__ void __launch_bounds__(128)
+k_sort_rows(int n, const int *__restrict__ rp, int *__restrict__ col, float *__restrict__ val,
+            int *__restrict__ long_rows, int *__restrict__ n_long)
+{
+    __shared__ unsigned long long sh[4][SORT_ROW_MAX];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long *a = sh[w];
+    for (int i = blockIdx.x * 4 + w; i < n; i += gridDim.x * 4) {
+        const int b = rp[i], len = rp[i + 1] - b;
+        if (len <= 1) continue;
+        if (len > SORT_ROW_MAX) {
+            if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
+            continue;
+        }
+        int m = 1;
+        while (m < len) m <<= 1;
+        for (int e = lane; e < m; e += 32)
+            a[e] = e < len ? ((unsigned long long)(unsigned int)col[b + e] << 32) | __float_as_uint(val[b + e])
+                           : ~0ull;
+        __syncwarp();
+        for (int k = 2; k <= m; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int e = lane; e < m; e += 32) {
+                    const int p = e ^ j;
+                    if (p > e) {
+                        const unsigned long long x = a[e], y = a[p];
+                        const bool up = (e & k) == 0;
+                        if ((x > y) == up) { a[e] = y; a[p] = x; }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        for (int e = lane; e < len; e += 32) {
+            col[b + e] = (int)(a[e] >> 32);
+            val[b + e] = __uint_as_float((unsigned int)(a[e] & 0xffffffffull));
+        }
+        __syncwarp();
+    }
+}
+
 // Conditional P_j|i by bisection on beta over min-shifted squared distances, FP64
 // (reference tsne_utils.c:952-1005): one warp per row; the search state is uniform
 // across the warp and every sum is a warp reduction.
@@ -566,6 +612,11 @@ void launch_row_copy(cudaStream_t st, int n, const int *ord, const int *inv, con
                      float *val_new)
 {
     k_row_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, ord, inv, rp_old, col_old, val_old, rp_new, col_new, val_new);
+}
+
+void launch_sort_rows(cudaStream_t st, int n, const int *rp, int *col, float *val, int *long_rows, int *n_long)
+{
+    k_sort_rows<<<ROW_GRID, 128, 0, st>>>(n, rp, col, val, long_rows, n_long);
 }
 
 void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist, double perplexity,

@@ -90,7 +90,7 @@ struct tsne_workspace {
     size_t vbytes = 0;              // bytes per point of the device vectors
 
     cudaStream_t st = nullptr;
-    DevBuf<int> rp, col, rp2, col2, len, inv, order, order2;
+    DevBuf<int> rp, col, rp2, col2, len, inv, order, order2, longrows;
     DevBuf<float> val, val2;
     DevBuf<unsigned char> Y, Yn, uY, gains, rep, frc, tmpv, Yconv;
     DevBuf<float> s;
@@ -241,18 +241,44 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     ws->col2.exact(std::max(total, 4));
     ws->val2.exact(std::max(total, 4));
-    DevBuf<int> colu;
-    DevBuf<float> valu;
-    colu.exact(std::max(total, 4));
-    valu.exact(std::max(total, 4));
-    launch_row_copy(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, colu.p, valu.p);
-    size_t sb = 0;
-    TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(nullptr, sb, colu.p, ws->col2.p, valu.p, ws->val2.p, total,
-                                                         n, ws->rp2.p, ws->rp2.p + 1, st));
-    ws->cub_tmp.ensure(sb + 256);
-    sb = ws->cub_tmp.cap;
-    TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(ws->cub_tmp.p, sb, colu.p, ws->col2.p, valu.p, ws->val2.p,
-                                                         total, n, ws->rp2.p, ws->rp2.p + 1, st));
+    launch_row_copy(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, ws->col2.p, ws->val2.p);
+    // rows sorted by new column: warp bitonic sort, then the few rows longer than its limit
+    // with a segmented sort over just those rows
+    ws->longrows.exact(n + 1);
+    TSNE_CUDA_CHECK(cudaMemsetAsync(ws->longrows.p + n, 0, sizeof(int), st));
+    launch_sort_rows(st, n, ws->rp2.p, ws->col2.p, ws->val2.p, ws->longrows.p, ws->longrows.p + n);
+    int n_long = 0;
+    TSNE_CUDA_CHECK(cudaMemcpyAsync(&n_long, ws->longrows.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (n_long > 0) {
+        std::vector<int> rows(n_long), rp_h(n + 1);
+        TSNE_CUDA_CHECK(cudaMemcpy(rows.data(), ws->longrows.p, sizeof(int) * n_long, cudaMemcpyDeviceToHost));
+        TSNE_CUDA_CHECK(cudaMemcpy(rp_h.data(), ws->rp2.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+        std::sort(rows.begin(), rows.end());
+        std::vector<int> beg(n_long), end(n_long);
+        int total_long = 0;
+        for (int r = 0; r < n_long; r++) { beg[r] = rp_h[rows[r]]; end[r] = rp_h[rows[r] + 1]; total_long += end[r] - beg[r]; }
+        DevBuf<int> dbeg, dend, kout;
+        DevBuf<float> vout;
+        dbeg.exact(n_long); dend.exact(n_long); kout.exact(total); vout.exact(total);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(dbeg.p, beg.data(), sizeof(int) * n_long, cudaMemcpyHostToDevice, st));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(dend.p, end.data(), sizeof(int) * n_long, cudaMemcpyHostToDevice, st));
+        size_t sb = 0;
+        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(nullptr, sb, ws->col2.p, kout.p, ws->val2.p, vout.p, total,
+                                                             n_long, dbeg.p, dend.p, st));
+        ws->cub_tmp.ensure(sb + 256);
+        sb = ws->cub_tmp.cap;
+        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(ws->cub_tmp.p, sb, ws->col2.p, kout.p, ws->val2.p, vout.p,
+                                                             total, n_long, dbeg.p, dend.p, st));
+        for (int r = 0; r < n_long; r++) {
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->col2.p + beg[r], kout.p + beg[r], sizeof(int) * (end[r] - beg[r]),
+                                            cudaMemcpyDeviceToDevice, st));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->val2.p + beg[r], vout.p + beg[r], sizeof(float) * (end[r] - beg[r]),
+                                            cudaMemcpyDeviceToDevice, st));
+        }
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+        (void)total_long;
+    }
     std::swap(ws->rp.p, ws->rp2.p); std::swap(ws->rp.cap, ws->rp2.cap);
     std::swap(ws->col.p, ws->col2.p); std::swap(ws->col.cap, ws->col2.cap);
     std::swap(ws->val.p, ws->val2.p); std::swap(ws->val.cap, ws->val2.cap);

@@ -69,6 +69,9 @@ void launch_row_len(cudaStream_t st, int n, const int *ord, const int *rp_old, i
 void launch_row_copy(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
                      const int *col_old, const float *val_old, const int *rp_new, int *col_new,
                      float *val_new);
+// sorts each row by column in place; rows longer than 1024 entries are appended to long_rows
+// (count in *n_long, which must start at 0) and left unsorted
+void launch_sort_rows(cudaStream_t st, int n, const int *rp, int *col, float *val, int *long_rows, int *n_long);
 void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist,
                  double perplexity, double *out);
 

@@ -1,0 +1,63 @@
+"""The Python host layer (parameter validation and mapping onto tsne_params_t); no GPU."""
+import numpy as np
+import pytest
+
+from tsne_h2pack import H2_DEFAULTS, TSNE, h2_defaults
+from tsne_h2pack.manifold import _resolve_n_jobs
+
+
+def test_h2_defaults_per_dimension():
+    assert h2_defaults(2) == dict(h2_tol=1e-2, h2_rebuild_freq=3, h2_rebuild_freq_early=10, h2_leaf_size=100)
+    assert h2_defaults(3)["h2_tol"] == 3e-2 and h2_defaults(5) == H2_DEFAULTS[3]
+    t = TSNE(n_components=3)
+    assert t.h2_tol == 3e-2 and t.h2_rebuild_freq == 3
+
+
+@pytest.mark.parametrize("kw", [dict(metric="cosine"), dict(init="spectral"), dict(method="bh"),
+                                dict(n_components=0), dict(perplexity=0), dict(learning_rate="fast"),
+                                dict(learning_rate=-1.0), dict(h2_rebuild_freq=0), dict(h2_leaf_size=0),
+                                dict(max_iter=0), dict(init=np.zeros((5, 3)))])
+def test_invalid_parameters_raise(kw):
+    with pytest.raises(ValueError):
+        TSNE(**kw)
+
+
+def test_param_mapping():
+    t = TSNE(method="exact", learning_rate="auto", h2_rebuild_freq_early=2, random_state=7, n_jobs=-1)
+    p = t._map_params_to_c_struct(n_samples=24000)
+    assert p.h2_rebuild_freq == 999999 and p.h2_tol == 1e-4
+    assert p.learning_rate == 2000.0
+    assert p.h2_rebuild_freq_early == 3         # never below the late frequency
+    assert p.random_seed == 7 and p.num_threads >= 1
+    p2 = TSNE(learning_rate=350.0)._map_params_to_c_struct(n_samples=100)
+    assert p2.learning_rate == 350.0 and p2.h2_rebuild_freq == 3 and p2.sklearn_compatible == 1
+
+
+def test_resolve_n_jobs():
+    import os
+    assert _resolve_n_jobs(None) == 1 and _resolve_n_jobs(0) == 1 and _resolve_n_jobs(4) == 4
+    assert _resolve_n_jobs(-1) == max(1, os.cpu_count() or 1)
+
+
+def test_validate_data():
+    t = TSNE(perplexity=30)
+    with pytest.raises(ValueError):
+        t._validate_data(np.zeros(5))
+    with pytest.raises(ValueError):
+        t._validate_data(np.zeros((10, 3)))          # perplexity >= n_samples
+    with pytest.raises(ValueError):
+        t._validate_data(np.full((100, 3), np.nan))
+
+
+def test_precomputed_graph_checks():
+    from scipy.sparse import csr_matrix
+    t = TSNE(metric="precomputed", perplexity=5, init="random")
+    with pytest.raises(ValueError):
+        t.fit_transform(np.zeros((10, 10)))          # dense
+    with pytest.raises(ValueError):
+        t.fit_transform(csr_matrix(np.ones((10, 12))))
+    G = csr_matrix(np.ones((10, 10)) - np.eye(10))
+    with pytest.raises(ValueError):
+        TSNE(metric="precomputed", perplexity=9, init="random").fit_transform(G)   # 9 neighbours <= 9
+    with pytest.raises(ValueError):
+        t.fit_transform(csr_matrix(-(np.ones((10, 10)) - np.eye(10))))            # negative distances

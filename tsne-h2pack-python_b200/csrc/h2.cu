@@ -96,28 +96,42 @@ __global__ void __launch_bounds__(256) k_bbox(int n, const Vec<D> *__restrict__ 
 
 // Root box from the bounding box (min / max are exact in any order), then the root node.
 template <int D>
-__global__ void k_root(int n, int L, int nblk, const double *__restrict__ part, TreeView tv)
+__global__ void __launch_bounds__(256) k_root(int n, int L, int nblk, const double *__restrict__ part, TreeView tv)
 {
-    if (threadIdx.x != 0) return;
+    __shared__ double slo[256][D], shi[256][D], sbad[256];
     double lo[D], hi[D], bad = 0.0;
     for (int k = 0; k < D; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
-    for (int b = 0; b < nblk; b++) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
         for (int k = 0; k < D; k++) {
             lo[k] = fmin(lo[k], part[(size_t)b * (2 * D + 1) + k]);
             hi[k] = fmax(hi[k], part[(size_t)b * (2 * D + 1) + D + k]);
         }
         bad += part[(size_t)b * (2 * D + 1) + 2 * D];
     }
+    for (int k = 0; k < D; k++) { slo[threadIdx.x][k] = lo[k]; shi[threadIdx.x][k] = hi[k]; }
+    sbad[threadIdx.x] = bad;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            for (int k = 0; k < D; k++) {
+                slo[threadIdx.x][k] = fmin(slo[threadIdx.x][k], slo[threadIdx.x + s][k]);
+                shi[threadIdx.x][k] = fmax(shi[threadIdx.x][k], shi[threadIdx.x + s][k]);
+            }
+            sbad[threadIdx.x] += sbad[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
     TreeInfo *info = tv.info;
     double ext = 0.0, ctr[D];
     for (int k = 0; k < D; k++) {
-        ctr[k] = 0.5 * (lo[k] + hi[k]);
-        const double e = 0.5 * (hi[k] - lo[k]);
+        ctr[k] = 0.5 * (slo[0][k] + shi[0][k]);
+        const double e = 0.5 * (shi[0][k] - slo[0][k]);
         if (e > ext) ext = e;
     }
     double R = MIN_HALF_WIDTH;
     for (int it = 0; it < 2100 && R < ext; it++) R *= 2.0;
-    info->nonfinite = bad > 0.0 ? 1 : 0;
+    info->nonfinite = sbad[0] > 0.0 ? 1 : 0;
     info->radius = R;
     for (int k = 0; k < 3; k++) info->corner[k] = k < D ? ctr[k] - R : 0.0;
     info->n_node = 1;
@@ -360,12 +374,21 @@ __device__ void process_target(const TreeView &tv, ListOut &lo, int t)
     }
 }
 
+// count pass, internal targets of one level (their NSET feeds the next level)
 template <int D>
 __global__ void __launch_bounds__(128) k_lists_level(int l, TreeView tv, ListOut lo)
 {
     const int lb = tv.info->level_begin[l], nl = tv.info->n_level_nodes[l];
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x)
-        process_target<D>(tv, lo, lb + j);
+        if (!tv.leaf[lb + j]) process_target<D>(tv, lo, lb + j);
+}
+
+// count pass, every leaf target (leaves need only their parent's NSET)
+template <int D>
+__global__ void __launch_bounds__(128) k_lists_leaves(int n_node, TreeView tv, ListOut lo)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x)
+        if (tv.leaf[t]) process_target<D>(tv, lo, t);
 }
 
 template <int D>
@@ -437,7 +460,7 @@ struct IdArgs {
     float *gA, *gnrm;
     int *gsel;
     void *gcand;
-    int mcap;
+    int mcap;      // candidate rows that fit the launch's shared memory
     float tol2;
 };
 
@@ -446,37 +469,39 @@ constexpr size_t id_smem_bytes(int mcap)
 {
     constexpr int P = Dim<D>::NPROXY, MAXR = Dim<D>::MAXR;
     return sizeof(float) * (size_t)P * D                 // proxies
-           + sizeof(float) * (size_t)MAXR * MAXR         // R11
            + sizeof(Vec<D>) * (size_t)mcap               // candidates
            + sizeof(float) * (size_t)mcap                // residual norms
-           + sizeof(int) * (size_t)mcap                  // pivot position per row
+           + sizeof(int) * (size_t)mcap                  // pivot position per row (-1: not selected)
            + sizeof(int) * (size_t)MAXR                  // pivot rows
-           + sizeof(float) * (size_t)P                   // current pivot direction
            + sizeof(float) * (size_t)mcap * (P + 1);     // the matrix (row stride P + 1)
 }
 
 // Interpolative decomposition of one node (one CTA): A = K(candidates - c, proxies),
 // column-pivoted Gram-Schmidt over the rows of A until the largest residual row norm is
 // <= tol * the largest initial one; U = [I ; R11^-1 R12]^T in candidate order.
-template <int D>
+// The dot products of every step go to the node's U rows (R12), and the column of R11 that
+// a step produces is stored in the pivot row of A, which no later step reads.
+// LEAVES = true: every leaf at level >= 2 (leaves depend on nothing), blockIdx.x counts
+// from the first node of level 2; false: the internal nodes of one level.
+template <int D, bool LEAVES>
 __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
 {
     constexpr int P = Dim<D>::NPROXY, PP = P + 1, MAXR = Dim<D>::MAXR;
     extern __shared__ __align__(16) unsigned char smraw[];
     const TreeView &tv = g.tv;
-    const int t = tv.info->level_begin[level] + blockIdx.x;
+    const int t = tv.info->level_begin[LEAVES ? MIN_ADM_LEVEL : level] + blockIdx.x;
+    if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) return;
+    const int lvl = tv.level[t];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const Vec<D> *xt = (const Vec<D> *)g.xt;
     Vec<D> *skel = (Vec<D> *)g.skel;
 
     unsigned char *ptr = smraw;
     float *prox = (float *)ptr; ptr += sizeof(float) * P * D;
-    float *R11 = (float *)ptr; ptr += sizeof(float) * MAXR * MAXR;
     Vec<D> *cand_s = (Vec<D> *)ptr; ptr += sizeof(Vec<D>) * g.mcap;
     float *nrm_s = (float *)ptr; ptr += sizeof(float) * g.mcap;
     int *selpos_s = (int *)ptr; ptr += sizeof(int) * g.mcap;
     int *sel = (int *)ptr; ptr += sizeof(int) * MAXR;
-    float *q = (float *)ptr; ptr += sizeof(float) * P;
     float *A_s = (float *)ptr;
 
     __shared__ float s_bv[ID_THREADS / 32];
@@ -484,9 +509,8 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     __shared__ int s_best, s_stop;
     __shared__ float s_n0;
 
-    const bool isleaf = tv.leaf[t] != 0;
     int m = 0;
-    if (isleaf) m = tv.end[t] - tv.start[t];
+    if (LEAVES) m = tv.end[t] - tv.start[t];
     else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
     const long long roff = g.rowoff[t];
     const bool glob = m > g.mcap;
@@ -496,12 +520,12 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     Vec<D> *cand = glob ? (Vec<D> *)g.gcand + roff : cand_s;
     float *U = g.U + roff * MAXR;
 
-    const double h = tv.info->radius / (double)(1LL << level);
+    const double h = tv.info->radius / (double)(1LL << lvl);
     for (int p = tid; p < P; p += ID_THREADS) proxy_point<D>(p, h, prox + p * D);
     float ctr[D];
     for (int k = 0; k < D; k++)
         ctr[k] = (float)(tv.info->corner[k] + (double)(2 * tv.ix[(size_t)t * 3 + k] + 1) * h);
-    if (isleaf) {
+    if (LEAVES) {
         for (int a = tid; a < m; a += ID_THREADS) cand[a] = xt[tv.start[t] + a];
     } else {
         for (int a = tid; a < m; a += ID_THREADS) {
@@ -518,11 +542,12 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
         float rel[D];
         for (int k = 0; k < D; k++) rel[k] = vget(x, k) - ctr[k];
         float s2 = 0.f;
+        float *row = A + (size_t)a * PP;
         for (int p = 0; p < P; p++) {
             float r2 = 0.f;
             for (int k = 0; k < D; k++) { const float df = rel[k] - prox[p * D + k]; r2 = fmaf(df, df, r2); }
             const float w = rkernel(r2);
-            A[(size_t)a * PP + p] = w;
+            row[p] = w;
             s2 = fmaf(w, w, s2);
         }
         nrm[a] = s2;
@@ -566,9 +591,9 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
         const int best = s_best;
         const float rr = sqrtf(nrm[best]);
         const float inv = 1.0f / rr;
-        for (int p = tid; p < P; p += ID_THREADS) q[p] = A[(size_t)best * PP + p] * inv;
-        for (int k = tid; k < r; k += ID_THREADS) R11[k * MAXR + r] = U[(size_t)best * MAXR + k];
-        if (tid == 0) { R11[r * MAXR + r] = rr; selpos[best] = r; sel[r] = best; }
+        float *q = A + (size_t)best * PP;
+        for (int p = tid; p < P; p += ID_THREADS) q[p] *= inv;
+        if (tid == 0) { selpos[best] = r; sel[r] = best; }
         __syncthreads();
         for (int a = tid; a < m; a += ID_THREADS) {
             if (selpos[a] >= 0) continue;
@@ -581,10 +606,15 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
             U[(size_t)a * MAXR + r] = dot;
         }
         __syncthreads();
+        // column r of R11 (R[0..r-1][best] from the earlier steps, then the norm) into the
+        // pivot row, which is dead from now on
+        for (int k = tid; k <= r; k += ID_THREADS) q[k] = k < r ? U[(size_t)best * MAXR + k] : rr;
         r++;
     }
+    __syncthreads();
     for (int k = tid; k < r; k += ID_THREADS) skel[(size_t)t * MAXR + k] = cand[sel[k]];
     if (tid == 0) g.rank[t] = r;
+    // R11[k][j] = A[sel[j]][k]
     for (int a = tid; a < m; a += ID_THREADS) {
         float *u = U + (size_t)a * MAXR;
         const int pos = selpos[a];
@@ -593,8 +623,8 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
         } else {
             for (int k = r - 1; k >= 0; k--) {
                 float acc = u[k];
-                for (int j = k + 1; j < r; j++) acc = fmaf(-R11[k * MAXR + j], u[j], acc);
-                u[k] = acc / R11[k * MAXR + k];
+                for (int j = k + 1; j < r; j++) acc = fmaf(-A[(size_t)sel[j] * PP + k], u[j], acc);
+                u[k] = acc / A[(size_t)sel[k] * PP + k];
             }
         }
     }
@@ -871,7 +901,9 @@ public:
         cap_node_ = std::max(1024, 4 * (n / 16) + 1024);
         alloc_nodes();
         nset_cap_ = Dim<D>::NSET;
-        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)id_smem_bytes<D>(id_mcap())));
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)id_smem_bytes<D>(id_mcap())));
     }
 
@@ -881,7 +913,7 @@ public:
         const int L = Dim<D>::L;
         for (int attempt = 0; attempt < 8; attempt++) {
             k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
-            k_root<D><<<1, 32, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
+            k_root<D><<<1, 256, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
             k_keys<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, L, (const Vec<D> *)Y, info_.p, keys_in_.p, idx_in_.p);
             size_t bytes = sort_bytes_;
             TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, bytes, keys_in_.p, keys_.p, idx_in_.p,
@@ -932,10 +964,12 @@ public:
             far_cnt_.exact(n_node_ + 1); near_cnt_.exact(n_node_ + 1);
             far_ptr_.exact(n_node_ + 2); near_ptr_.exact(n_node_ + 2);
             ListOut lo = list_out(0);
-            for (int l = 0; l <= max_level_; l++) {
+            for (int l = 0; l < max_level_; l++) {
                 k_lists_level<D><<<grid_for(I.n_level_nodes[l], 128, 148 * 8), 128, 0, st_>>>(l, view(), lo);
                 launches_++;
             }
+            k_lists_leaves<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
+            launches_++;
             scan_exclusive(far_cnt_.p, far_ptr_.p, n_node_);
             scan_exclusive(near_cnt_.p, near_ptr_.p, n_node_);
             rowcap_.exact(n_node_ + 1);
@@ -977,12 +1011,19 @@ public:
             gsel_.ensure(std::max<long long>(hrows_, 1));
             gcand_.ensure(std::max<long long>(hrows_, 1));
         }
-        IdArgs ia{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mcap,
-                  (float)((tol * ID_TOL_FACTOR) * (tol * ID_TOL_FACTOR))};
-        const size_t smem = id_smem_bytes<D>(mcap);
-        for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
+        const float tol2 = (float)((tol * ID_TOL_FACTOR) * (tol * ID_TOL_FACTOR));
+        // leaves: one launch, shared memory sized for the largest leaf
+        const int mleaf = std::max(1, std::min(stats_.max_leaf, mcap));
+        IdArgs il{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mleaf, tol2};
+        const int first = I.level_begin[MIN_ADM_LEVEL];
+        k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
+        launches_++;
+        // internal nodes, bottom-up (their candidates are the children's skeletons)
+        IdArgs ia = il;
+        ia.mcap = mcap;
+        for (int l = max_level_ - 1; l >= MIN_ADM_LEVEL; l--) {
             const int nl = I.n_level_nodes[l];
-            if (nl > 0) { k_id<D><<<nl, ID_THREADS, smem, st_>>>(l, ia); launches_++; }
+            if (nl > 0) { k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia); launches_++; }
         }
         built_ = true;
         rank_stats_valid_ = false;

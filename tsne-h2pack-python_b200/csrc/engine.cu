@@ -759,6 +759,10 @@ int tsne_run(tsne_workspace_t *ws)
     const int rc = tsne_run_range(ws, 0, ws->params.n_iter);
     ws->n_launch = ws->n_launch - l0;
     if (ws->params.verbose) printf("\nOptimization complete\n");
+    if (env_int("TSNE_H2_TIMERS", 0) && ws->h2) {
+        printf("H2REBUILDS %d\n", ws->n_rebuild);
+        try { ws->h2->flush_timers(); } catch (const CudaError &) {}
+    }
     if (rc == 0 && ws->prof && !ws->prof_file.empty()) tsne_write_profiling_data(ws, ws->prof_file.c_str());
     return rc;
 }

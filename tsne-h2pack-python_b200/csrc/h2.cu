@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -462,6 +463,7 @@ struct IdArgs {
     void *gcand;
     int mcap;      // candidate rows that fit the launch's shared memory
     float tol2;
+    float4 *y0;    // upward-pass coefficients of [1 | Y], computed right after the basis
 };
 
 template <int D>
@@ -627,6 +629,31 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
                 u[k] = acc / A[(size_t)sel[k] * PP + k];
             }
         }
+    }
+    // upward pass of this node: y0[t] = U^T (the leaf's [1 | x] | the children's y0)
+    __syncthreads();
+    for (int k = tid; k < r; k += ID_THREADS) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (LEAVES) {
+            for (int a = 0; a < m; a++) {
+                const float w = U[(size_t)a * MAXR + k];
+                const Vec<D> x = cand[a];
+                acc.x += w;
+                acc.y = fmaf(w, vget(x, 0), acc.y);
+                acc.z = fmaf(w, vget(x, 1), acc.z);
+                if (D == 3) acc.w = fmaf(w, vget(x, 2), acc.w);
+            }
+        } else {
+            int a = 0;
+            for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++)
+                for (int kk = 0; kk < g.rank[c]; kk++, a++) {
+                    const float w = U[(size_t)a * MAXR + k];
+                    const float4 y = g.y0[(size_t)c * MAXR + kk];
+                    acc.x = fmaf(w, y.x, acc.x); acc.y = fmaf(w, y.y, acc.y);
+                    acc.z = fmaf(w, y.z, acc.z); acc.w = fmaf(w, y.w, acc.w);
+                }
+        }
+        g.y0[(size_t)t * MAXR + k] = acc;
     }
 }
 
@@ -811,15 +838,19 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
 }
 
 // downward pass, one warp per node of `level`: children's y1 / the leaf's points += U_t y1[t]
-template <int D>
+// LEAVES = false: the internal nodes of `level` (run top-down); true: every leaf at level >= 2
+// (after all internal levels)
+template <int D, bool LEAVES>
 __global__ void __launch_bounds__(256) k_down(int level, ProdArgs g)
 {
     constexpr int MAXR = Dim<D>::MAXR;
     const TreeView &tv = g.tv;
-    const int lb = tv.info->level_begin[level], nl = tv.info->n_level_nodes[level];
+    const int lb = tv.info->level_begin[level];
+    const int nl = LEAVES ? tv.info->n_node - lb : tv.info->n_level_nodes[level];
     const int lane = threadIdx.x & 31;
     for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nl; j += (gridDim.x * blockDim.x) >> 5) {
         const int t = lb + j;
+        if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) continue;
         const int r = g.rank[t];
         const float *U = g.U + g.rowoff[t] * MAXR;
         float4 yr[MAXR / 32];
@@ -911,6 +942,7 @@ public:
     {
         leaf_size_ = leaf_size;
         const int L = Dim<D>::L;
+        cudaEvent_t t_tree = mark_begin();
         for (int attempt = 0; attempt < 8; attempt++) {
             k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
             k_root<D><<<1, 256, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
@@ -925,7 +957,7 @@ public:
             bool overflow = false;
             for (;;) {
                 for (int l = launched; l < want; l++) {
-                    k_split<D><<<grid_for(cap_node_, 256, 148 * 8), 256, 0, st_>>>(l, view());
+                    k_split<D><<<148, 256, 0, st_>>>(l, view());
                     k_emit<D><<<1, 1024, 0, st_>>>(l, view());
                     launches_ += 2;
                 }
@@ -948,6 +980,7 @@ public:
             }
             break;
         }
+        mark_end(t_tree, 0);
         const TreeInfo &I = *hinfo_.p;
         n_node_ = I.n_node;
         max_level_ = I.max_level;
@@ -958,6 +991,7 @@ public:
         if (max_level_ <= 2) { built_ = false; return 1; }
 
         // interaction lists: count per level, scan, write
+        cudaEvent_t t_lists = mark_begin();
         for (int attempt = 0; attempt < 4; attempt++) {
             nset_.exact((size_t)n_node_ * nset_cap_);
             nset_cnt_.exact(n_node_);
@@ -995,7 +1029,9 @@ public:
             launches_++;
         }
 
+        mark_end(t_lists, 1);
         // bases, bottom-up
+        cudaEvent_t t_bases = mark_begin();
         constexpr int MAXR = Dim<D>::MAXR, P = Dim<D>::NPROXY;
         rank_.exact(n_node_);
         TSNE_CUDA_CHECK(cudaMemsetAsync(rank_.p, 0, sizeof(int) * n_node_, st_));
@@ -1014,7 +1050,8 @@ public:
         const float tol2 = (float)((tol * ID_TOL_FACTOR) * (tol * ID_TOL_FACTOR));
         // leaves: one launch, shared memory sized for the largest leaf
         const int mleaf = std::max(1, std::min(stats_.max_leaf, mcap));
-        IdArgs il{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mleaf, tol2};
+        IdArgs il{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mleaf, tol2,
+                  y0_.p};
         const int first = I.level_begin[MIN_ADM_LEVEL];
         k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
         launches_++;
@@ -1025,7 +1062,9 @@ public:
             const int nl = I.n_level_nodes[l];
             if (nl > 0) { k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia); launches_++; }
         }
+        mark_end(t_bases, 2);
         built_ = true;
+        y0_from_build_ = true;
         rank_stats_valid_ = false;
         return 0;
     }
@@ -1033,9 +1072,11 @@ public:
     void product_force(void *F, DevScalars *sc, double *partials, int keep_rep) override
     {
         run_product();
+        cudaEvent_t t_force = mark_begin();
         k_split_out<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, yp_.p, s_.p, (Vec<D> *)v_.p);
         launch_z_force<D>(st_, n_, xt_.p, s_.p, v_.p, perm_.p, F, sc, partials, 1, keep_rep);
         launches_ += 3;
+        mark_end(t_force, 6);
     }
 
     void product_host(std::vector<float> &s, std::vector<float> &v) override
@@ -1126,8 +1167,51 @@ public:
 
     long long launches() const override { return launches_; }
 
+    // TSNE_H2_TIMERS=1: device time per phase (CUDA events on the stream), summed over builds
+    // and products until flush_timers() prints them
+    void flush_timers() override
+    {
+        if (!timing_) return;
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        static const char *names[N_PHASE] = {"tree", "lists", "bases+up", "far", "near", "down", "force"};
+        for (auto &m : marks_) {
+            float ms = 0.f;
+            TSNE_CUDA_CHECK(cudaEventElapsedTime(&ms, m.a, m.b));
+            phase_ms_[m.phase] += ms;
+            cudaEventDestroy(m.a);
+            cudaEventDestroy(m.b);
+        }
+        marks_.clear();
+        printf("H2TIMERS");
+        for (int i = 0; i < N_PHASE; i++) printf(" %s=%.3f", names[i], phase_ms_[i] * 1e-3);
+        printf(" (s)\n");
+        fflush(stdout);
+        for (double &x : phase_ms_) x = 0.0;
+    }
+
 private:
     static constexpr int BBOX_BLOCKS = 148 * 2;
+    static constexpr int N_PHASE = 7;
+    struct Mark { cudaEvent_t a, b; int phase; };
+    bool timing_ = getenv("TSNE_H2_TIMERS") && atoi(getenv("TSNE_H2_TIMERS")) != 0;
+    std::vector<Mark> marks_;
+    double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t mark_begin()
+    {
+        cudaEvent_t e = nullptr;
+        if (!timing_) return e;
+        TSNE_CUDA_CHECK(cudaEventCreate(&e));
+        TSNE_CUDA_CHECK(cudaEventRecord(e, st_));
+        return e;
+    }
+    void mark_end(cudaEvent_t a, int phase)
+    {
+        if (!timing_) return;
+        cudaEvent_t b;
+        TSNE_CUDA_CHECK(cudaEventCreate(&b));
+        TSNE_CUDA_CHECK(cudaEventRecord(b, st_));
+        marks_.push_back({a, b, phase});
+    }
 
     static int id_mcap()
     {
@@ -1193,18 +1277,29 @@ private:
         g.y0 = y0_.p; g.y1 = y1_.p; g.yp = yp_.p;
         g.far_ptr = far_ptr_.p; g.far_idx = far_idx_.p; g.near_ptr = near_ptr_.p; g.near_idx = near_idx_.p;
         const TreeInfo &I = *hinfo_.p;
-        for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
-            const int nl = I.n_level_nodes[l];
-            if (nl > 0) { k_up<D><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
+        if (xin != nullptr || !y0_from_build_) {
+            for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
+                const int nl = I.n_level_nodes[l];
+                if (nl > 0) { k_up<D><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
+            }
         }
+        y0_from_build_ = y0_from_build_ && xin == nullptr;
         const int first = I.level_begin[MIN_ADM_LEVEL];
+        cudaEvent_t t_far = mark_begin();
         k_far_c<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(first, n_node_, g);
+        mark_end(t_far, 3);
+        cudaEvent_t t_near = mark_begin();
         k_near<D><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
+        mark_end(t_near, 4);
         launches_ += 2;
-        for (int l = MIN_ADM_LEVEL; l <= max_level_; l++) {
+        cudaEvent_t t_down = mark_begin();
+        for (int l = MIN_ADM_LEVEL; l < max_level_; l++) {
             const int nl = I.n_level_nodes[l];
-            if (nl > 0) { k_down<D><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
+            if (nl > 0) { k_down<D, false><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
         }
+        k_down<D, true><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(MIN_ADM_LEVEL, g);
+        launches_++;
+        mark_end(t_down, 5);
     }
 
     int n_;
@@ -1213,6 +1308,7 @@ private:
     int cap_node_ = 0, nset_cap_ = 0;
     int n_node_ = 0, max_level_ = 0, last_max_level_ = 0;
     bool built_ = false;
+    bool y0_from_build_ = false;   // y0 holds U^T [1 | Y] of the last build
     mutable bool rank_stats_valid_ = false;
     mutable H2Stats stats_;
     long long launches_ = 0;

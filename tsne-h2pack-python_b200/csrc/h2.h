@@ -38,6 +38,8 @@ public:
     virtual void copy_lists(int *far_ptr, int *far_idx, int *near_ptr, int *near_idx) = 0;
     virtual void copy_ranks(int *rank) = 0;
     virtual long long launches() const = 0;
+    // prints and clears the per-phase device times gathered under TSNE_H2_TIMERS=1
+    virtual void flush_timers() = 0;
 };
 
 std::unique_ptr<H2Matrix> make_h2_matrix(int d, int n, cudaStream_t st);

@@ -109,7 +109,7 @@ __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)
 // Fixed launch geometry of the row-parallel kernels: results are reduced block-wise in a
 // fixed order, so the grid must not depend on the device's occupancy.
 constexpr int ROW_BLOCK = 256;        // 8 warps
-constexpr int ROW_GRID = 148 * 4;     // one wave of 4 blocks per SM on a 148-SM B200
+constexpr int ROW_GRID = 148 * 8;     // 8 blocks per SM on a 148-SM B200
 constexpr int RED_BLOCK = 256;
 
 }  // namespace tsne

@@ -11,6 +11,7 @@
 //   renumbering ................ src/tsne_reorder.c:112-167
 //   perplexity calibration ..... src/tsne_utils.c:952-1105
 #include <math.h>
+#include <stdlib.h>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -136,7 +137,7 @@ __device__ __forceinline__ void chunk_acc(const Vec<D> &yi, const Vec<D> *__rest
 
 template <int D>
 __global__ void __launch_bounds__(ROW_BLOCK, 4)
-k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+k_attr_update_stream(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
               const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
               Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
               float exag4, float mom, float lr, double *__restrict__ partials)
@@ -206,6 +207,63 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
             }
             i = ni; pos = npos; e = ne; c4 = nc4; p4 = np4;
             yi = nyi; u_i = nu; g_i = ng; f_i = nf;
+        }
+    }
+    block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
+}
+
+// Block-contiguous variant: block b owns rows [b R, (b + 1) R); its 8 warps take rows
+// b R + w, b R + w + 8, ... so that at any moment they work on 8 consecutive rows, and over
+// time the block sweeps one contiguous region, whose neighbours (the points are renumbered
+// in tree order) keep hitting the same L1 lines. Lanes 1-3 fetch the row's update operands
+// while the warp streams the row.
+template <int D>
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+              float exag4, float mom, float lr, double *__restrict__ partials)
+{
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int use_rep = (rep != nullptr) ? *rep_flag : 0;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
+    double acc[D];
+    for (int k = 0; k < D; k++) acc[k] = 0.0;
+    for (int i = r0 + wib; i < r1; i += ROW_BLOCK / 32) {
+        const Vec<D> yi = Y[i];
+        Vec<D> opnd = vzero<D>();
+        if (lane == 1) opnd = uY[i];
+        else if (lane == 2) opnd = gains[i];
+        else if (lane == 3 && use_rep) opnd = rep[i];
+        float a[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) a[k] = 0.f;
+        row_attr<D>(rp[i], rp[i + 1], lane, yi, col, val, Y, a);
+        Vec<D> u = vzero<D>(), g = vzero<D>(), r = vzero<D>();
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            vset(u, k, __shfl_sync(0xffffffffu, vget(opnd, k), 1));
+            vset(g, k, __shfl_sync(0xffffffffu, vget(opnd, k), 2));
+            vset(r, k, __shfl_sync(0xffffffffu, vget(opnd, k), 3));
+        }
+        if (lane == 0) {
+            Vec<D> yn = yi;
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                const float gk = exag4 * a[k] - vget(r, k);
+                const float uk = vget(u, k);
+                float gain = (uk * gk < 0.f) ? vget(g, k) + 0.2f : vget(g, k) * 0.8f;
+                gain = fmaxf(gain, 0.01f);
+                const float un = mom * uk - lr * (gk * gain);
+                vset(g, k, gain);
+                vset(u, k, un);
+                vset(yn, k, vget(yi, k) + un);
+                acc[k] += (double)vget(yn, k);
+            }
+            uY[i] = u;
+            gains[i] = g;
+            Yn[i] = yn;
         }
     }
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
@@ -575,9 +633,15 @@ void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, c
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
                         const int *rep_flag, float exag4, float mom, float lr, double *partials)
 {
-    k_attr_update<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
+    static const int variant = getenv("TSNE_ATTR_VARIANT") ? atoi(getenv("TSNE_ATTR_VARIANT")) : 0;
+    if (variant == 1)
+        k_attr_update_stream<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
+    else
+        k_attr_update<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
 }
 
 template <int D>

@@ -1055,6 +1055,8 @@ public:
         const int first = I.level_begin[MIN_ADM_LEVEL];
         k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
         launches_++;
+        mark_end(t_bases, 2);
+        t_bases = mark_begin();
         // internal nodes, bottom-up (their candidates are the children's skeletons)
         IdArgs ia = il;
         ia.mcap = mcap;
@@ -1062,7 +1064,7 @@ public:
             const int nl = I.n_level_nodes[l];
             if (nl > 0) { k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia); launches_++; }
         }
-        mark_end(t_bases, 2);
+        mark_end(t_bases, 7);
         built_ = true;
         y0_from_build_ = true;
         rank_stats_valid_ = false;
@@ -1173,7 +1175,8 @@ public:
     {
         if (!timing_) return;
         TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
-        static const char *names[N_PHASE] = {"tree", "lists", "bases+up", "far", "near", "down", "force"};
+        static const char *names[N_PHASE] = {"tree", "lists", "leaf_bases", "far", "near", "down", "force",
+                                             "internal_bases"};
         for (auto &m : marks_) {
             float ms = 0.f;
             TSNE_CUDA_CHECK(cudaEventElapsedTime(&ms, m.a, m.b));
@@ -1191,11 +1194,11 @@ public:
 
 private:
     static constexpr int BBOX_BLOCKS = 148 * 2;
-    static constexpr int N_PHASE = 7;
+    static constexpr int N_PHASE = 8;
     struct Mark { cudaEvent_t a, b; int phase; };
     bool timing_ = getenv("TSNE_H2_TIMERS") && atoi(getenv("TSNE_H2_TIMERS")) != 0;
     std::vector<Mark> marks_;
-    double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0};
+    double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaEvent_t mark_begin()
     {
         cudaEvent_t e = nullptr;

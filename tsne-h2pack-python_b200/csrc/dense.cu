@@ -118,26 +118,13 @@ __device__ __forceinline__ void reduce_partials(const double *__restrict__ part,
 //   g = 4 exag sum_j p_ij (y_i - y_j) / (1 + |y_i - y_j|^2) - F_rep
 //   gain: +0.2 if uY * g < 0 else * 0.8, floor 0.01; uY = mom uY - lr gain g; Y += uY
 // Ynext is a separate buffer because other warps still gather the old Y.
-//
-// Each warp owns a contiguous range of rows, i.e. a contiguous stretch of the padded CSR,
-// and walks it in 128-entry chunks (4 entries per lane, two 128-bit loads). The loads of the
-// next chunk, and the next row's coordinates and update operands, are issued before the
-// current chunk's gathers are consumed, so every warp keeps a P chunk in flight while it
-// waits on Y.
 // ---------------------------------------------------------------------------------
+// Rows are dealt to warps round-robin (row i to warp i mod W), so that at any moment all
+// warps of the device stream one window of P: the HBM traffic stays within a few MB of
+// consecutive rows. Lanes 1-3 fetch the row's update operands while the warp streams it.
 template <int D>
-__device__ __forceinline__ void chunk_acc(const Vec<D> &yi, const Vec<D> *__restrict__ Y, const int4 &c4,
-                                          const float4 &p4, float (&a)[D])
-{
-    attr_acc<D>(yi, Y, c4.x, p4.x, a);
-    attr_acc<D>(yi, Y, c4.y, p4.y, a);
-    attr_acc<D>(yi, Y, c4.z, p4.z, a);
-    attr_acc<D>(yi, Y, c4.w, p4.w, a);
-}
-
-template <int D>
-__global__ void __launch_bounds__(ROW_BLOCK, 4)
-k_attr_update_stream(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
               const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
               Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
               float exag4, float mom, float lr, double *__restrict__ partials)
@@ -146,91 +133,9 @@ k_attr_update_stream(int n, const int *__restrict__ rp, const int *__restrict__ 
     const int warp = blockIdx.x * (ROW_BLOCK / 32) + (threadIdx.x >> 5);
     const int nwarp = gridDim.x * (ROW_BLOCK / 32);
     const int use_rep = (rep != nullptr) ? *rep_flag : 0;
-    const int per = (n + nwarp - 1) / nwarp;
-    const int r0 = min(n, warp * per), r1 = min(n, r0 + per);
     double acc[D];
     for (int k = 0; k < D; k++) acc[k] = 0.0;
-    if (r0 < r1) {
-        int i = r0;
-        int e = rp[i + 1];
-        int pos = rp[i];
-        Vec<D> yi = Y[i];
-        Vec<D> u_i = vzero<D>(), g_i = vzero<D>(), f_i = vzero<D>();
-        if (lane == 0) { u_i = uY[i]; g_i = gains[i]; if (use_rep) f_i = rep[i]; }
-        int4 c4 = make_int4(0, 0, 0, 0);
-        float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (pos + 4 * lane < e) { c4 = ld_stream_i4(col + pos + 4 * lane); p4 = ld_stream_f4(val + pos + 4 * lane); }
-        float a[D];
-        for (int k = 0; k < D; k++) a[k] = 0.f;
-        while (true) {
-            // position of the next chunk: the rest of this row, else the next row
-            const bool row_ends = pos + 128 >= e;
-            const int ni = row_ends ? i + 1 : i;
-            const bool more = ni < r1;
-            const int npos = row_ends ? e : pos + 128;
-            const int ne = (row_ends && more) ? rp[ni + 1] : e;
-            int4 nc4 = make_int4(0, 0, 0, 0);
-            float4 np4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (more && npos + 4 * lane < ne) {
-                nc4 = ld_stream_i4(col + npos + 4 * lane);
-                np4 = ld_stream_f4(val + npos + 4 * lane);
-            }
-            Vec<D> nyi = yi, nu = u_i, ng = g_i, nf = f_i;
-            if (row_ends && more) {
-                nyi = Y[ni];
-                if (lane == 0) { nu = uY[ni]; ng = gains[ni]; if (use_rep) nf = rep[ni]; }
-            }
-            chunk_acc<D>(yi, Y, c4, p4, a);
-            if (row_ends) {
-#pragma unroll
-                for (int k = 0; k < D; k++) a[k] = warp_sum(a[k]);
-                if (lane == 0) {
-                    Vec<D> yn = yi;
-#pragma unroll
-                    for (int k = 0; k < D; k++) {
-                        const float gk = exag4 * a[k] - vget(f_i, k);
-                        const float uk = vget(u_i, k);
-                        float gain = (uk * gk < 0.f) ? vget(g_i, k) + 0.2f : vget(g_i, k) * 0.8f;
-                        gain = fmaxf(gain, 0.01f);
-                        const float un = mom * uk - lr * (gk * gain);
-                        vset(g_i, k, gain);
-                        vset(u_i, k, un);
-                        vset(yn, k, vget(yi, k) + un);
-                        acc[k] += (double)vget(yn, k);
-                    }
-                    uY[i] = u_i;
-                    gains[i] = g_i;
-                    Yn[i] = yn;
-                }
-                for (int k = 0; k < D; k++) a[k] = 0.f;
-                if (!more) break;
-            }
-            i = ni; pos = npos; e = ne; c4 = nc4; p4 = np4;
-            yi = nyi; u_i = nu; g_i = ng; f_i = nf;
-        }
-    }
-    block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
-}
-
-// Block-contiguous variant: block b owns rows [b R, (b + 1) R); its 8 warps take rows
-// b R + w, b R + w + 8, ... so that at any moment they work on 8 consecutive rows, and over
-// time the block sweeps one contiguous region, whose neighbours (the points are renumbered
-// in tree order) keep hitting the same L1 lines. Lanes 1-3 fetch the row's update operands
-// while the warp streams the row.
-template <int D>
-__global__ void __launch_bounds__(ROW_BLOCK)
-k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
-              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
-              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
-              float exag4, float mom, float lr, double *__restrict__ partials)
-{
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int use_rep = (rep != nullptr) ? *rep_flag : 0;
-    const int per = (n + gridDim.x - 1) / gridDim.x;
-    const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
-    double acc[D];
-    for (int k = 0; k < D; k++) acc[k] = 0.0;
-    for (int i = r0 + wib; i < r1; i += ROW_BLOCK / 32) {
+    for (int i = warp; i < n; i += nwarp) {
         const Vec<D> yi = Y[i];
         Vec<D> opnd = vzero<D>();
         if (lane == 1) opnd = uY[i];
@@ -633,15 +538,9 @@ void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, c
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
                         const int *rep_flag, float exag4, float mom, float lr, double *partials)
 {
-    static const int variant = getenv("TSNE_ATTR_VARIANT") ? atoi(getenv("TSNE_ATTR_VARIANT")) : 0;
-    if (variant == 1)
-        k_attr_update_stream<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
-    else
-        k_attr_update<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
+    k_attr_update<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
 }
 
 template <int D>

@@ -657,6 +657,197 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     }
 }
 
+// Register-resident ID (2D): thread `tid` owns candidate rows tid + ID_THREADS * j (j < RPT),
+// each a row of A = K(candidate - c, proxies) held in registers; the pivot row of a step is
+// normalised by its owner and broadcast through shared memory. Per step every thread
+// projects the pivot out of its rows, refreshes their norms, records the dot products in
+// the node's U rows (R12) and proposes its best remaining row; two barriers per step.
+// The column of R11 produced by a step goes to shared memory. Same decomposition, same
+// stopping rule and same U layout as k_id.
+template <bool LEAVES, int RPT>
+__global__ void __launch_bounds__(ID_THREADS, RPT == 1 ? 4 : 2) k_id_reg(int level, IdArgs g)
+{
+    constexpr int P = Dim<2>::NPROXY, MAXR = Dim<2>::MAXR, NW = ID_THREADS / 32;
+    using V2 = float2;
+    const TreeView &tv = g.tv;
+    const int t = tv.info->level_begin[LEAVES ? MIN_ADM_LEVEL : level] + blockIdx.x;
+    if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) return;
+    const int lvl = tv.level[t];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const V2 *xt = (const V2 *)g.xt;
+    V2 *skel = (V2 *)g.skel;
+
+    __shared__ float prox[P * 2];
+    __shared__ float qsh[P];
+    __shared__ float R11[MAXR * MAXR];
+    __shared__ float s_bv[2][NW];
+    __shared__ int s_bi[2][NW];
+    __shared__ float s_rr;
+    __shared__ int s_crank[8], s_cfirst;
+
+    int m = 0;
+    if (LEAVES) m = tv.end[t] - tv.start[t];
+    else {
+        if (tid == 0) s_cfirst = tv.fchild[t];
+        for (int c = 0; c < tv.nchild[t]; c++) {
+            const int rc = g.rank[tv.fchild[t] + c];
+            if (tid == 0) s_crank[c] = rc;
+            m += rc;
+        }
+    }
+    const long long roff = g.rowoff[t];
+    float *U = g.U + roff * MAXR;
+    const double h = tv.info->radius / (double)(1LL << lvl);
+    for (int p = tid; p < P; p += ID_THREADS) proxy_point<2>(p, h, prox + p * 2);
+    const float cx = (float)(tv.info->corner[0] + (double)(2 * tv.ix[(size_t)t * 3 + 0] + 1) * h);
+    const float cy = (float)(tv.info->corner[1] + (double)(2 * tv.ix[(size_t)t * 3 + 1] + 1) * h);
+    __syncthreads();
+
+    float row[RPT][P];
+    float nrm[RPT];
+    V2 x[RPT];
+    int pos[RPT];
+    float lmax = 0.f;
+#pragma unroll
+    for (int j = 0; j < RPT; j++) {
+        const int a = tid + ID_THREADS * j;
+        pos[j] = a < m ? -1 : -2;
+        x[j] = make_float2(0.f, 0.f);
+        if (a < m) {
+            if (LEAVES) x[j] = xt[tv.start[t] + a];
+            else {
+                int c = 0, aa = a;
+                while (aa >= s_crank[c]) { aa -= s_crank[c]; c++; }
+                x[j] = skel[(size_t)(s_cfirst + c) * MAXR + aa];
+            }
+        }
+        const float rx = x[j].x - cx, ry = x[j].y - cy;
+        float s2 = 0.f;
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            const float dx = rx - prox[2 * p], dy = ry - prox[2 * p + 1];
+            const float w = a < m ? rkernel(fmaf(dx, dx, dy * dy)) : 0.f;
+            row[j][p] = w;
+            s2 = fmaf(w, w, s2);
+        }
+        nrm[j] = a < m ? s2 : -1.f;
+        lmax = fmaxf(lmax, s2);
+    }
+    // largest initial norm, and the first pivot proposal
+    float bv = -1.f;
+    int bi = INT_MAX;
+#pragma unroll
+    for (int j = 0; j < RPT; j++)
+        if (nrm[j] > bv) { bv = nrm[j]; bi = tid + ID_THREADS * j; }
+    for (int o = 16; o > 0; o >>= 1) {
+        lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    __shared__ float s_lmax[NW];
+    if (lane == 0) { s_lmax[wid] = lmax; s_bv[0][wid] = bv; s_bi[0][wid] = bi; }
+    __syncthreads();
+    float n0 = 0.f;
+    for (int w = 0; w < NW; w++) n0 = fmaxf(n0, s_lmax[w]);
+    const float stop2 = g.tol2 * n0;
+    const int rmax = min(min(m, P), MAXR);
+    int r = 0, buf = 0;
+    while (r < rmax) {
+        // every thread reads the same partials: the same pivot everywhere
+        float v = s_bv[buf][0];
+        int best = s_bi[buf][0];
+        for (int w = 1; w < NW; w++)
+            if (s_bv[buf][w] > v || (s_bv[buf][w] == v && s_bi[buf][w] < best)) { v = s_bv[buf][w]; best = s_bi[buf][w]; }
+        if (best == INT_MAX || !(v > stop2) || !(v > 0.f)) break;
+        const int owner = best % ID_THREADS, jb = best / ID_THREADS;
+        if (tid == owner) {
+#pragma unroll
+            for (int j = 0; j < RPT; j++)
+                if (j == jb) {
+                    const float rr = sqrtf(nrm[j]);
+                    const float inv = 1.0f / rr;
+#pragma unroll
+                    for (int p = 0; p < P; p++) qsh[p] = row[j][p] * inv;
+                    s_rr = rr;
+                    pos[j] = r;
+                    nrm[j] = -1.f;
+                }
+        }
+        for (int k = tid; k < r; k += ID_THREADS) R11[k * MAXR + r] = U[(size_t)best * MAXR + k];
+        __syncthreads();
+        if (tid == 0) R11[r * MAXR + r] = s_rr;
+        bv = -1.f;
+        bi = INT_MAX;
+#pragma unroll
+        for (int j = 0; j < RPT; j++) {
+            if (pos[j] != -1) continue;
+            float dot = 0.f;
+#pragma unroll
+            for (int p = 0; p < P; p++) dot = fmaf(qsh[p], row[j][p], dot);
+            float s2 = 0.f;
+#pragma unroll
+            for (int p = 0; p < P; p++) { row[j][p] = fmaf(-dot, qsh[p], row[j][p]); s2 = fmaf(row[j][p], row[j][p], s2); }
+            nrm[j] = s2;
+            U[(size_t)(tid + ID_THREADS * j) * MAXR + r] = dot;
+            if (s2 > bv) { bv = s2; bi = tid + ID_THREADS * j; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        buf ^= 1;
+        if (lane == 0) { s_bv[buf][wid] = bv; s_bi[buf][wid] = bi; }
+        r++;
+        __syncthreads();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < RPT; j++)
+        if (pos[j] >= 0) skel[(size_t)t * MAXR + pos[j]] = x[j];
+    if (tid == 0) g.rank[t] = r;
+#pragma unroll
+    for (int j = 0; j < RPT; j++) {
+        const int a = tid + ID_THREADS * j;
+        if (a >= m) continue;
+        float *u = U + (size_t)a * MAXR;
+        if (pos[j] >= 0) {
+            for (int k = 0; k < r; k++) u[k] = (k == pos[j]) ? 1.f : 0.f;
+        } else {
+            for (int k = r - 1; k >= 0; k--) {
+                float acc = u[k];
+                for (int jj = k + 1; jj < r; jj++) acc = fmaf(-R11[k * MAXR + jj], u[jj], acc);
+                u[k] = acc / R11[k * MAXR + k];
+            }
+        }
+    }
+    __syncthreads();
+    // upward pass of this node: y0[t] = U^T (the leaf's [1 | x] | the children's y0)
+    for (int k = tid; k < r; k += ID_THREADS) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (LEAVES) {
+            for (int a = 0; a < m; a++) {
+                const float w = U[(size_t)a * MAXR + k];
+                const V2 xa = xt[tv.start[t] + a];
+                acc.x += w;
+                acc.y = fmaf(w, xa.x, acc.y);
+                acc.z = fmaf(w, xa.y, acc.z);
+            }
+        } else {
+            int a = 0;
+            for (int c = 0; c < tv.nchild[t]; c++)
+                for (int kk = 0; kk < s_crank[c]; kk++, a++) {
+                    const float w = U[(size_t)a * MAXR + k];
+                    const float4 y = g.y0[(size_t)(s_cfirst + c) * MAXR + kk];
+                    acc.x = fmaf(w, y.x, acc.x); acc.y = fmaf(w, y.y, acc.y);
+                    acc.z = fmaf(w, y.z, acc.z); acc.w = fmaf(w, y.w, acc.w);
+                }
+        }
+        g.y0[(size_t)t * MAXR + k] = acc;
+    }
+}
+
 // ---------------------------------------------------------------------------------
 // product kernels
 // ---------------------------------------------------------------------------------
@@ -1053,7 +1244,10 @@ public:
         IdArgs il{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mleaf, tol2,
                   y0_.p};
         const int first = I.level_begin[MIN_ADM_LEVEL];
-        k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
+        if (D == 2 && stats_.max_leaf <= ID_THREADS)
+            k_id_reg<true, 1><<<n_node_ - first, ID_THREADS, 0, st_>>>(MIN_ADM_LEVEL, il);
+        else
+            k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
         launches_++;
         mark_end(t_bases, 2);
         t_bases = mark_begin();
@@ -1062,7 +1256,10 @@ public:
         ia.mcap = mcap;
         for (int l = max_level_ - 1; l >= MIN_ADM_LEVEL; l--) {
             const int nl = I.n_level_nodes[l];
-            if (nl > 0) { k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia); launches_++; }
+            if (nl == 0) continue;
+            if (D == 2) k_id_reg<false, 2><<<nl, ID_THREADS, 0, st_>>>(l, ia);
+            else k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia);
+            launches_++;
         }
         mark_end(t_bases, 7);
         built_ = true;

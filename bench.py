@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--save-embedding", default=None)
     ap.add_argument("--graph-cache", default=None, help="npz file holding the k-NN graph and P")
+    ap.add_argument("--profile-csv", default=None, help="write the per-iteration stage CSV of the last step")
     return ap.parse_args()
 
 
@@ -151,6 +152,9 @@ def ours(args, rank, world, local):
     def step():
         """One e2e step through the C ABI; returns (wall s, device run s, attr ms, attr launches, launches)."""
         prm = params_for(be, n, args.iters)
+        if args.profile_csv:
+            prm.enable_profiling = 1
+            prm.profiling_output_file = args.profile_csv.encode()
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         Pc = scipy_csr_to_c_sparse_matrix(P, lib)

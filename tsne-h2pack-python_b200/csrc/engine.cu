@@ -393,7 +393,9 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
             if (prof) stage_event(ws, evpool, evused);
             if (next_reorder_due(ws, iter, reorder_iters, n_reorder) && ws->h2_valid) {
                 while (ws->next_reorder < n_reorder && iter >= reorder_iters[ws->next_reorder]) ws->next_reorder++;
+                const double t0 = wall_sec();
                 renumber(ws, ws->h2->perm_device());
+                if (env_int("TSNE_H2_TIMERS", 0)) printf("RENUMBER iter %d %.1f ms\n", iter, 1e3 * (wall_sec() - t0));
             }
             if (rebuild_h2(ws) != 0) {
                 fprintf(stderr, "ERROR: Failed to rebuild H2 matrix at iteration %d\n", iter);

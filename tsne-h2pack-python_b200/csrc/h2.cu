@@ -22,6 +22,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstdlib>
 #include <vector>
@@ -1134,6 +1135,7 @@ public:
         leaf_size_ = leaf_size;
         const int L = Dim<D>::L;
         cudaEvent_t t_tree = mark_begin();
+        sec_begin();
         for (int attempt = 0; attempt < 8; attempt++) {
             k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
             k_root<D><<<1, 256, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
@@ -1172,6 +1174,7 @@ public:
             break;
         }
         mark_end(t_tree, 0);
+        sec_end("tree");
         const TreeInfo &I = *hinfo_.p;
         n_node_ = I.n_node;
         max_level_ = I.max_level;
@@ -1221,6 +1224,7 @@ public:
         }
 
         mark_end(t_lists, 1);
+        sec_end("lists");
         // bases, bottom-up
         cudaEvent_t t_bases = mark_begin();
         constexpr int MAXR = Dim<D>::MAXR, P = Dim<D>::NPROXY;
@@ -1262,6 +1266,8 @@ public:
             launches_++;
         }
         mark_end(t_bases, 7);
+        if (timing_) TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        sec_end("bases");
         built_ = true;
         y0_from_build_ = true;
         rank_stats_valid_ = false;
@@ -1403,6 +1409,17 @@ private:
         TSNE_CUDA_CHECK(cudaEventCreate(&e));
         TSNE_CUDA_CHECK(cudaEventRecord(e, st_));
         return e;
+    }
+    // host wall time of one build section; sections slower than 10 ms are reported
+    std::chrono::steady_clock::time_point sec_t0_;
+    void sec_begin() { if (timing_) sec_t0_ = std::chrono::steady_clock::now(); }
+    void sec_end(const char *name)
+    {
+        if (!timing_) return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - sec_t0_).count();
+        if (ms > 10.0) printf("H2SLOW %s %.1f ms (n_node %d, max_leaf %d, far %d, near %d, nset_cap %d, cap_node %d)\n", name, ms,
+                              n_node_, stats_.max_leaf, htot_[0], htot_[1], nset_cap_, cap_node_);
+        sec_t0_ = std::chrono::steady_clock::now();
     }
     void mark_end(cudaEvent_t a, int phase)
     {

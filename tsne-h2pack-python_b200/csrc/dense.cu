@@ -413,12 +413,13 @@ __global__ void k_row_len(int n, const int *__restrict__ ord, const int *__restr
     }
 }
 
-// Renumbered rows (reference tsne_reorder.c:112-167): new row k is old row ord[k] with
-// columns mapped through inv; the rows are sorted by column afterwards.
+// Renumbered rows (reference tsne_reorder.c:112-167): new row k is old row ord[k] with its
+// columns mapped through inv. Emits, for the first transpose, key = new column and value =
+// (new row << 32 | value bits), entries grouped by new row in increasing order.
 __global__ void k_row_copy(int n, const int *__restrict__ ord, const int *__restrict__ inv,
                            const int *__restrict__ rp_old, const int *__restrict__ col_old,
                            const float *__restrict__ val_old, const int *__restrict__ rp_new,
-                           int *__restrict__ col_new, float *__restrict__ val_new)
+                           unsigned int *__restrict__ key, unsigned long long *__restrict__ pack)
 {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -426,55 +427,32 @@ __global__ void k_row_copy(int n, const int *__restrict__ ord, const int *__rest
     for (int k = warp; k < n; k += nwarp) {
         const int i = ord[k], b = rp_old[i], len = rp_old[i + 1] - b, o = rp_new[k];
         for (int e = lane; e < len; e += 32) {
-            col_new[o + e] = inv[col_old[b + e]];
-            val_new[o + e] = val_old[b + e];
+            key[o + e] = (unsigned int)inv[col_old[b + e]];
+            pack[o + e] = ((unsigned long long)(unsigned int)k << 32) | __float_as_uint(val_old[b + e]);
         }
     }
 }
 
-// Sort every row of a padded CSR by column (the renumbered P, reference tsne_reorder.c
-// leaves each row sorted by its new column numbers): one warp per row, bitonic sort of the
-// row in shared memory (rows up to SORT_ROW_MAX entries); longer rows are listed for the
-// caller, which sorts them separately.
-constexpr int SORT_ROW_MAX = 1024;
-__global__ void __launch_bounds__(128)
-k_sort_rows(int n, const int *__restrict__ rp, int *__restrict__ col, float *__restrict__ val,
-            int *__restrict__ long_rows, int *__restrict__ n_long)
+// After the first (stable) sort by new column c: key = new row, value = (c << 32 | bits)
+__global__ void k_swap_pack(long long nnz, const unsigned int *__restrict__ key_in,
+                            const unsigned long long *__restrict__ pack_in, unsigned int *__restrict__ key_out,
+                            unsigned long long *__restrict__ pack_out)
 {
-    __shared__ unsigned long long sh[4][SORT_ROW_MAX];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    unsigned long long *a = sh[w];
-    for (int i = blockIdx.x * 4 + w; i < n; i += gridDim.x * 4) {
-        const int b = rp[i], len = rp[i + 1] - b;
-        if (len <= 1) continue;
-        if (len > SORT_ROW_MAX) {
-            if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
-            continue;
-        }
-        int m = 1;
-        while (m < len) m <<= 1;
-        for (int e = lane; e < m; e += 32)
-            a[e] = e < len ? ((unsigned long long)(unsigned int)col[b + e] << 32) | __float_as_uint(val[b + e])
-                           : ~0ull;
-        __syncwarp();
-        for (int k = 2; k <= m; k <<= 1) {
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int e = lane; e < m; e += 32) {
-                    const int p = e ^ j;
-                    if (p > e) {
-                        const unsigned long long x = a[e], y = a[p];
-                        const bool up = (e & k) == 0;
-                        if ((x > y) == up) { a[e] = y; a[p] = x; }
-                    }
-                }
-                __syncwarp();
-            }
-        }
-        for (int e = lane; e < len; e += 32) {
-            col[b + e] = (int)(a[e] >> 32);
-            val[b + e] = __uint_as_float((unsigned int)(a[e] & 0xffffffffull));
-        }
-        __syncwarp();
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long p = pack_in[e];
+        key_out[e] = (unsigned int)(p >> 32);
+        pack_out[e] = ((unsigned long long)key_in[e] << 32) | (p & 0xffffffffull);
+    }
+}
+
+// After the second sort by new row: entries are grouped by row and sorted by column
+__global__ void k_unpack(long long nnz, const unsigned long long *__restrict__ pack, int *__restrict__ col,
+                         float *__restrict__ val)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long p = pack[e];
+        col[e] = (int)(p >> 32);
+        val[e] = __uint_as_float((unsigned int)(p & 0xffffffffull));
     }
 }
 
@@ -622,15 +600,21 @@ void launch_row_len(cudaStream_t st, int n, const int *ord, const int *rp_old, i
 }
 
 void launch_row_copy(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
-                     const int *col_old, const float *val_old, const int *rp_new, int *col_new,
-                     float *val_new)
+                     const int *col_old, const float *val_old, const int *rp_new, unsigned int *key,
+                     unsigned long long *pack)
 {
-    k_row_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, ord, inv, rp_old, col_old, val_old, rp_new, col_new, val_new);
+    k_row_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, ord, inv, rp_old, col_old, val_old, rp_new, key, pack);
 }
 
-void launch_sort_rows(cudaStream_t st, int n, const int *rp, int *col, float *val, int *long_rows, int *n_long)
+void launch_swap_pack(cudaStream_t st, long long nnz, const unsigned int *key_in, const unsigned long long *pack_in,
+                      unsigned int *key_out, unsigned long long *pack_out)
 {
-    k_sort_rows<<<ROW_GRID, 128, 0, st>>>(n, rp, col, val, long_rows, n_long);
+    k_swap_pack<<<148 * 16, 256, 0, st>>>(nnz, key_in, pack_in, key_out, pack_out);
+}
+
+void launch_unpack(cudaStream_t st, long long nnz, const unsigned long long *pack, int *col, float *val)
+{
+    k_unpack<<<148 * 16, 256, 0, st>>>(nnz, pack, col, val);
 }
 
 void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist, double perplexity,

@@ -90,7 +90,10 @@ struct tsne_workspace {
     size_t vbytes = 0;              // bytes per point of the device vectors
 
     cudaStream_t st = nullptr;
-    DevBuf<int> rp, col, rp2, col2, len, inv, order, order2, longrows;
+    DevBuf<int> rp, col, rp2, col2, len, inv, order, order2;
+    DevBuf<unsigned int> rkey[2];              // renumbering: sort keys
+    DevBuf<unsigned long long> rpack[2];       // renumbering: (index, value) pairs
+    long long padded_nnz = 0;
     DevBuf<float> val, val2;
     DevBuf<unsigned char> Y, Yn, uY, gains, rep, frc, tmpv, Yconv;
     DevBuf<float> s;
@@ -151,6 +154,7 @@ void upload_P(tsne_workspace *ws)
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     ws->col.exact(std::max(padded, 4));
     ws->val.exact(std::max(padded, 4));
+    ws->padded_nnz = padded;
     k_pad_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, rp0.p, ci0.p, pv0.p, ws->rp.p, ws->col.p, ws->val.p);
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     ws->n_launch += 3;
@@ -220,10 +224,17 @@ int rebuild_h2(tsne_workspace *ws)
     return 0;
 }
 
+// Renumbering (reference tsne_reorder.c:112-167): new point k = old point ord[k]. P is
+// renumbered like the reference does it, by two transposes whose stable ordering leaves every
+// row sorted by its new column: entries are emitted in new-row order with key = new column,
+// stably radix-sorted (grouping them by column, rows ascending inside a group), re-keyed by
+// row and sorted again. Then every per-point array is permuted and the cumulative order
+// updated. No host synchronisation.
 template <int D>
 void renumber_impl(tsne_workspace *ws, const int *ord_dev)
 {
     const int n = ws->n;
+    const long long nnz = ws->padded_nnz;
     cudaStream_t st = ws->st;
     ws->inv.exact(n);
     ws->len.exact(n + 1);
@@ -236,49 +247,28 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     ws->cub_tmp.ensure(bytes + 256);
     bytes = ws->cub_tmp.cap;
     TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(ws->cub_tmp.p, bytes, ws->len.p, ws->rp2.p + 1, n, st));
-    int total = 0;
-    TSNE_CUDA_CHECK(cudaMemcpyAsync(&total, ws->rp.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
-    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
-    ws->col2.exact(std::max(total, 4));
-    ws->val2.exact(std::max(total, 4));
-    launch_row_copy(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, ws->col2.p, ws->val2.p);
-    // rows sorted by new column: warp bitonic sort, then the few rows longer than its limit
-    // with a segmented sort over just those rows
-    ws->longrows.exact(n + 1);
-    TSNE_CUDA_CHECK(cudaMemsetAsync(ws->longrows.p + n, 0, sizeof(int), st));
-    launch_sort_rows(st, n, ws->rp2.p, ws->col2.p, ws->val2.p, ws->longrows.p, ws->longrows.p + n);
-    int n_long = 0;
-    TSNE_CUDA_CHECK(cudaMemcpyAsync(&n_long, ws->longrows.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
-    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
-    if (n_long > 0) {
-        std::vector<int> rows(n_long), rp_h(n + 1);
-        TSNE_CUDA_CHECK(cudaMemcpy(rows.data(), ws->longrows.p, sizeof(int) * n_long, cudaMemcpyDeviceToHost));
-        TSNE_CUDA_CHECK(cudaMemcpy(rp_h.data(), ws->rp2.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
-        std::sort(rows.begin(), rows.end());
-        std::vector<int> beg(n_long), end(n_long);
-        int total_long = 0;
-        for (int r = 0; r < n_long; r++) { beg[r] = rp_h[rows[r]]; end[r] = rp_h[rows[r] + 1]; total_long += end[r] - beg[r]; }
-        DevBuf<int> dbeg, dend, kout;
-        DevBuf<float> vout;
-        dbeg.exact(n_long); dend.exact(n_long); kout.exact(total); vout.exact(total);
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(dbeg.p, beg.data(), sizeof(int) * n_long, cudaMemcpyHostToDevice, st));
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(dend.p, end.data(), sizeof(int) * n_long, cudaMemcpyHostToDevice, st));
-        size_t sb = 0;
-        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(nullptr, sb, ws->col2.p, kout.p, ws->val2.p, vout.p, total,
-                                                             n_long, dbeg.p, dend.p, st));
-        ws->cub_tmp.ensure(sb + 256);
-        sb = ws->cub_tmp.cap;
-        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortPairs(ws->cub_tmp.p, sb, ws->col2.p, kout.p, ws->val2.p, vout.p,
-                                                             total, n_long, dbeg.p, dend.p, st));
-        for (int r = 0; r < n_long; r++) {
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->col2.p + beg[r], kout.p + beg[r], sizeof(int) * (end[r] - beg[r]),
-                                            cudaMemcpyDeviceToDevice, st));
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->val2.p + beg[r], vout.p + beg[r], sizeof(float) * (end[r] - beg[r]),
-                                            cudaMemcpyDeviceToDevice, st));
-        }
-        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
-        (void)total_long;
-    }
+    ws->rkey[0].exact(nnz); ws->rkey[1].exact(nnz);
+    ws->rpack[0].exact(nnz); ws->rpack[1].exact(nnz);
+    launch_row_copy(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, ws->rkey[0].p,
+                    ws->rpack[0].p);
+    int bits = 1;
+    while ((1LL << bits) < n) bits++;
+    size_t sb = 0;
+    TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, sb, ws->rkey[0].p, ws->rkey[1].p, ws->rpack[0].p,
+                                                    ws->rpack[1].p, nnz, 0, bits, st));
+    ws->cub_tmp.ensure(sb + 256);
+    sb = ws->cub_tmp.cap;
+    // first transpose: group by new column (rows stay ascending: the sort is stable)
+    TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(ws->cub_tmp.p, sb, ws->rkey[0].p, ws->rkey[1].p, ws->rpack[0].p,
+                                                    ws->rpack[1].p, nnz, 0, bits, st));
+    launch_swap_pack(st, nnz, ws->rkey[1].p, ws->rpack[1].p, ws->rkey[0].p, ws->rpack[0].p);
+    // second transpose: group by new row, columns ascending
+    sb = ws->cub_tmp.cap;
+    TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(ws->cub_tmp.p, sb, ws->rkey[0].p, ws->rkey[1].p, ws->rpack[0].p,
+                                                    ws->rpack[1].p, nnz, 0, bits, st));
+    ws->col2.exact(std::max<long long>(nnz, 4));
+    ws->val2.exact(std::max<long long>(nnz, 4));
+    launch_unpack(st, nnz, ws->rpack[1].p, ws->col2.p, ws->val2.p);
     std::swap(ws->rp.p, ws->rp2.p); std::swap(ws->rp.cap, ws->rp2.cap);
     std::swap(ws->col.p, ws->col2.p); std::swap(ws->col.cap, ws->col2.cap);
     std::swap(ws->val.p, ws->val2.p); std::swap(ws->val.cap, ws->val2.cap);
@@ -295,8 +285,7 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     std::swap(ws->order.p, ws->order2.p);
     std::swap(ws->order.cap, ws->order2.cap);
     ws->has_order = true;
-    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
-    ws->n_launch += 14;
+    ws->n_launch += 16;
 }
 
 void renumber(tsne_workspace *ws, const int *ord_dev)

@@ -387,8 +387,9 @@ __global__ void __launch_bounds__(128) k_lists_level(int l, TreeView tv, ListOut
 
 // count pass, every leaf target (leaves need only their parent's NSET)
 template <int D>
-__global__ void __launch_bounds__(128) k_lists_leaves(int n_node, TreeView tv, ListOut lo)
+__global__ void __launch_bounds__(128) k_lists_leaves(TreeView tv, ListOut lo)
 {
+    const int n_node = tv.info->n_node;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x)
         if (tv.leaf[t]) process_target<D>(tv, lo, t);
 }
@@ -403,9 +404,10 @@ __global__ void __launch_bounds__(128) k_lists_write(int n_node, TreeView tv, Li
 // rows of each node's interpolation matrix: a leaf's points, or (upper bound) the
 // children's skeletons; nodes above MIN_ADM_LEVEL are not compressed
 template <int D>
-__global__ void k_rowcap(int n_node, TreeView tv, int *__restrict__ rowcap)
+__global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap)
 {
     constexpr int NCH = 1 << D;
+    const int n_node = tv.info->n_node;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x) {
         int r = 0;
         if (tv.level[t] >= MIN_ADM_LEVEL) r = tv.leaf[t] ? tv.end[t] - tv.start[t] : NCH * Dim<D>::MAXR;
@@ -1122,8 +1124,8 @@ public:
         sort_bytes_ = b1;
         cub_tmp_.exact(std::max(b1, b2) + 256);
         cap_node_ = std::max(1024, 4 * (n / 16) + 1024);
-        alloc_nodes();
         nset_cap_ = Dim<D>::NSET;
+        alloc_nodes();
         TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)id_smem_bytes<D>(id_mcap())));
         TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1136,45 +1138,60 @@ public:
         const int L = Dim<D>::L;
         cudaEvent_t t_tree = mark_begin();
         sec_begin();
-        for (int attempt = 0; attempt < 8; attempt++) {
-            k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
-            k_root<D><<<1, 256, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
-            k_keys<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, L, (const Vec<D> *)Y, info_.p, keys_in_.p, idx_in_.p);
-            size_t bytes = sort_bytes_;
-            TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, bytes, keys_in_.p, keys_.p, idx_in_.p,
-                                                            perm_.p, n_, 0, D * L, st_));
-            k_gather<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, perm_.p, (const Vec<D> *)Y, (Vec<D> *)xt_.p);
-            launches_ += 5 + 4;
-            int launched = 0;
-            int want = std::min(L + 1, std::max(6, last_max_level_ + 2));
-            bool overflow = false;
-            for (;;) {
-                for (int l = launched; l < want; l++) {
-                    k_split<D><<<148, 256, 0, st_>>>(l, view());
-                    k_emit<D><<<1, 1024, 0, st_>>>(l, view());
-                    launches_ += 2;
-                }
-                launched = want;
-                TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
-                TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
-                const TreeInfo &I = *hinfo_.p;
-                if (I.nonfinite) return -1;
-                if (I.pad[0]) { overflow = true; break; }
-                if (launched <= L && launched < 31 && I.n_level_nodes[launched] > 0) {
-                    want = std::min(L + 1, launched + 4);
-                    continue;
-                }
-                break;
+        // One batch: root box, keys, sort, tree levels and the counting pass of the interaction
+        // lists (kernels read the level and node counts on the device; scans run over the node
+        // capacity, whose unused tail counts are zero), then a single synchronisation reads the
+        // tree, the list totals and the basis rows. A deeper tree than the launched levels, a
+        // full node table or a full inadmissible-source set are caught there and redone.
+        int launched = 0;
+        for (int attempt = 0; attempt < 12; attempt++) {
+            if (launched == 0) {
+                k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
+                k_root<D><<<1, 256, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
+                k_keys<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, L, (const Vec<D> *)Y, info_.p, keys_in_.p, idx_in_.p);
+                size_t bytes = sort_bytes_;
+                TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, bytes, keys_in_.p, keys_.p, idx_in_.p,
+                                                                perm_.p, n_, 0, D * L, st_));
+                k_gather<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, perm_.p, (const Vec<D> *)Y, (Vec<D> *)xt_.p);
+                launches_ += 5 + 4;
             }
-            if (overflow) {
+            const int want = std::min(L + 1, std::max(launched + 4, std::max(6, last_max_level_ + 2)));
+            for (int l = launched; l < want; l++) {
+                k_split<D><<<148, 256, 0, st_>>>(l, view());
+                k_emit<D><<<1, 1024, 0, st_>>>(l, view());
+                launches_ += 2;
+            }
+            launched = want;
+            launch_list_counts(want);
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + cap_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+            const TreeInfo &I = *hinfo_.p;
+            if (I.nonfinite) return -1;
+            if (I.pad[0]) {   // node table full: grow and start over
                 cap_node_ *= 2;
                 alloc_nodes();
+                launched = 0;
                 continue;
+            }
+            if (launched <= L && launched < 31 && I.n_level_nodes[launched] > 0) continue;   // deeper tree
+            if (I.nset_overflow) {   // inadmissible-source set full: grow, recount
+                nset_cap_ *= 2;
+                alloc_lists();
+                launch_list_counts(launched);
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + cap_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
+                TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+                if (hinfo_.p->nset_overflow && attempt < 11) continue;
             }
             break;
         }
         mark_end(t_tree, 0);
-        sec_end("tree");
+        sec_end("tree+counts");
         const TreeInfo &I = *hinfo_.p;
         n_node_ = I.n_node;
         max_level_ = I.max_level;
@@ -1184,35 +1201,7 @@ public:
         stats_.max_leaf = I.max_leaf;
         if (max_level_ <= 2) { built_ = false; return 1; }
 
-        // interaction lists: count per level, scan, write
         cudaEvent_t t_lists = mark_begin();
-        for (int attempt = 0; attempt < 4; attempt++) {
-            nset_.exact((size_t)n_node_ * nset_cap_);
-            nset_cnt_.exact(n_node_);
-            far_cnt_.exact(n_node_ + 1); near_cnt_.exact(n_node_ + 1);
-            far_ptr_.exact(n_node_ + 2); near_ptr_.exact(n_node_ + 2);
-            ListOut lo = list_out(0);
-            for (int l = 0; l < max_level_; l++) {
-                k_lists_level<D><<<grid_for(I.n_level_nodes[l], 128, 148 * 8), 128, 0, st_>>>(l, view(), lo);
-                launches_++;
-            }
-            k_lists_leaves<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
-            launches_++;
-            scan_exclusive(far_cnt_.p, far_ptr_.p, n_node_);
-            scan_exclusive(near_cnt_.p, near_ptr_.p, n_node_);
-            rowcap_.exact(n_node_ + 1);
-            rowoff_.exact(n_node_ + 2);
-            k_rowcap<D><<<grid_for(n_node_, 256), 256, 0, st_>>>(n_node_, view(), rowcap_.p);
-            scan_exclusive_ll(rowcap_.p, rowoff_.p, n_node_);
-            launches_ += 4;
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + n_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + n_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + n_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
-            TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
-            if (hinfo_.p->nset_overflow) { nset_cap_ *= 2; continue; }
-            break;
-        }
         stats_.n_far = htot_[0];
         stats_.n_near = htot_[1];
         far_idx_.ensure(std::max(1, htot_[0]));
@@ -1222,9 +1211,8 @@ public:
             k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
             launches_++;
         }
-
         mark_end(t_lists, 1);
-        sec_end("lists");
+
         // bases, bottom-up
         cudaEvent_t t_bases = mark_begin();
         constexpr int MAXR = Dim<D>::MAXR, P = Dim<D>::NPROXY;
@@ -1267,11 +1255,43 @@ public:
         }
         mark_end(t_bases, 7);
         if (timing_) TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
-        sec_end("bases");
+        sec_end("lists+bases");
         built_ = true;
         y0_from_build_ = true;
         rank_stats_valid_ = false;
         return 0;
+    }
+
+    // counting pass of the lists for levels [0, levels) plus every leaf target, the pointer
+    // scans and the basis row offsets, all over the node capacity
+    void launch_list_counts(int levels)
+    {
+        TSNE_CUDA_CHECK(cudaMemsetAsync(far_cnt_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
+        TSNE_CUDA_CHECK(cudaMemsetAsync(near_cnt_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
+        TSNE_CUDA_CHECK(cudaMemsetAsync(rowcap_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
+        TSNE_CUDA_CHECK(cudaMemsetAsync(&info_.p->nset_overflow, 0, sizeof(int), st_));
+        ListOut lo = list_out(0);
+        for (int l = 0; l < levels; l++) {
+            k_lists_level<D><<<148 * 2, 128, 0, st_>>>(l, view(), lo);
+            launches_++;
+        }
+        k_lists_leaves<D><<<148 * 8, 128, 0, st_>>>(view(), lo);
+        k_rowcap<D><<<148 * 4, 256, 0, st_>>>(view(), rowcap_.p);
+        scan_exclusive(far_cnt_.p, far_ptr_.p, cap_node_);
+        scan_exclusive(near_cnt_.p, near_ptr_.p, cap_node_);
+        scan_exclusive_ll(rowcap_.p, rowoff_.p, cap_node_);
+        launches_ += 5;
+    }
+
+    void alloc_lists()
+    {
+        const size_t c = cap_node_;
+        nset_.exact(c * nset_cap_);
+        nset_cnt_.exact(c + 1);
+        far_cnt_.exact(c + 1); near_cnt_.exact(c + 1);
+        far_ptr_.exact(c + 2); near_ptr_.exact(c + 2);
+        rowcap_.exact(c + 1);
+        rowoff_.exact(c + 2);
     }
 
     void product_force(void *F, DevScalars *sc, double *partials, int keep_rep) override
@@ -1443,6 +1463,7 @@ private:
         start_.exact(c); end_.exact(c); level_.exact(c); parent_.exact(c); fchild_.exact(c);
         nchild_.exact(c); leaf_.exact(c); ix_.exact(3 * c); nch_.exact(c);
         cb_.exact(c * ((1 << D) + 1));
+        alloc_lists();
     }
 
     TreeView view()

@@ -208,6 +208,26 @@ TSNE_API int tsne_get_timing(tsne_workspace_t *workspace, double *run_ms, double
 /* Number of H2 rebuilds and kernel launches issued by the last tsne_run / tsne_run_range */
 TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, long long *n_launch);
 
+/* ---- no-allocation entry point (no counterpart in the reference) ----
+ *
+ * Exact repulsive force of an embedding, for callers that must not allocate device memory
+ * (a process serving under a fixed, pre-carved memory budget, code where the implicit
+ * device synchronisation of an allocation is not acceptable, or hosts with their own
+ * allocator). Y (input) and F (output) are device arrays of n_point x low_dim floats,
+ * point-major (x0, y0[, z0], x1, ...); Z is a device double receiving the normalisation.
+ * F_i = (4 / Z) sum_{j != i} (1 + |y_i - y_j|^2)^-2 (y_i - y_j), Z from the identity of the
+ * reference (src/tsne_h2pack.c:555-590) on the exact sums.
+ *
+ * The scratch lives in a file-scope __device__ array sized for at most 65536 points (about
+ * 1 MB, held by every device that loads the library until the process exits); larger
+ * n_point is rejected with -1. The first call on a device looks up that array's device
+ * address (once per device, with the device current), so make the first call on each device
+ * before any stream capture. All calls on a device share the array: calls that overlap on
+ * the GPU race on it. stream: a cudaStream_t, or NULL for the legacy default stream.
+ * Returns 0 on success, -1 on bad arguments, -2 on a CUDA error. Asynchronous on `stream`. */
+TSNE_API int tsne_exact_repulsion_static(const float *Y, int n_point, int low_dim, float *F, double *Z,
+                                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif

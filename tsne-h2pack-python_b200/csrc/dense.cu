@@ -119,9 +119,11 @@ __device__ __forceinline__ void reduce_partials(const double *__restrict__ part,
 //   gain: +0.2 if uY * g < 0 else * 0.8, floor 0.01; uY = mom uY - lr gain g; Y += uY
 // Ynext is a separate buffer because other warps still gather the old Y.
 // ---------------------------------------------------------------------------------
-// Rows are dealt to warps round-robin (row i to warp i mod W), so that at any moment all
-// warps of the device stream one window of P: the HBM traffic stays within a few MB of
-// consecutive rows. Lanes 1-3 fetch the row's update operands while the warp streams it.
+// Rows are dealt round-robin to half-warps (row i to half-warp i mod H), so that at any
+// moment all warps of the device stream one window of P (the HBM traffic stays within a few
+// MB of consecutive rows) and every warp has two independent rows, i.e. two streams of P
+// loads and Y gathers, in flight. A half-warp reads 64 entries per step (4 per lane, two
+// 128-bit loads); lanes 1-3 of the half fetch the row's update operands meanwhile.
 template <int D>
 __global__ void __launch_bounds__(ROW_BLOCK)
 k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
@@ -129,30 +131,50 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
               Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
               float exag4, float mom, float lr, double *__restrict__ partials)
 {
-    const int lane = threadIdx.x & 31;
-    const int warp = blockIdx.x * (ROW_BLOCK / 32) + (threadIdx.x >> 5);
-    const int nwarp = gridDim.x * (ROW_BLOCK / 32);
+    const int lane = threadIdx.x & 31, hl = lane & 15;
+    const int half = (blockIdx.x * ROW_BLOCK + threadIdx.x) >> 4;
+    const int nhalf = (gridDim.x * ROW_BLOCK) >> 4;
     const int use_rep = (rep != nullptr) ? *rep_flag : 0;
     double acc[D];
     for (int k = 0; k < D; k++) acc[k] = 0.0;
-    for (int i = warp; i < n; i += nwarp) {
-        const Vec<D> yi = Y[i];
-        Vec<D> opnd = vzero<D>();
-        if (lane == 1) opnd = uY[i];
-        else if (lane == 2) opnd = gains[i];
-        else if (lane == 3 && use_rep) opnd = rep[i];
+    // both halves of a warp run the same number of rounds, so full-warp shuffles stay legal
+    const int rounds = (n + nhalf - 1) / nhalf;
+    for (int rd = 0; rd < rounds; rd++) {
+        const int i = half + rd * nhalf;
+        const bool live = i < n;
+        Vec<D> yi = vzero<D>(), opnd = vzero<D>();
+        int b = 0, e = 0;
+        if (live) {
+            yi = Y[i];
+            b = rp[i];
+            e = rp[i + 1];
+            if (hl == 1) opnd = uY[i];
+            else if (hl == 2) opnd = gains[i];
+            else if (hl == 3 && use_rep) opnd = rep[i];
+        }
         float a[D];
 #pragma unroll
         for (int k = 0; k < D; k++) a[k] = 0.f;
-        row_attr<D>(rp[i], rp[i + 1], lane, yi, col, val, Y, a);
+        for (int base = b + 4 * hl; base < e; base += 64) {
+            const int4 c4 = ld_stream_i4(col + base);
+            const float4 p4 = ld_stream_f4(val + base);
+            attr_acc<D>(yi, Y, c4.x, p4.x, a);
+            attr_acc<D>(yi, Y, c4.y, p4.y, a);
+            attr_acc<D>(yi, Y, c4.z, p4.z, a);
+            attr_acc<D>(yi, Y, c4.w, p4.w, a);
+        }
+#pragma unroll
+        for (int k = 0; k < D; k++)
+            for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+        const int src = lane & 16;
         Vec<D> u = vzero<D>(), g = vzero<D>(), r = vzero<D>();
 #pragma unroll
         for (int k = 0; k < D; k++) {
-            vset(u, k, __shfl_sync(0xffffffffu, vget(opnd, k), 1));
-            vset(g, k, __shfl_sync(0xffffffffu, vget(opnd, k), 2));
-            vset(r, k, __shfl_sync(0xffffffffu, vget(opnd, k), 3));
+            vset(u, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 1));
+            vset(g, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 2));
+            vset(r, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 3));
         }
-        if (lane == 0) {
+        if (live && hl == 0) {
             Vec<D> yn = yi;
 #pragma unroll
             for (int k = 0; k < D; k++) {
@@ -171,6 +193,8 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
             Yn[i] = yn;
         }
     }
+    // lanes 0 and 16 of each warp hold partial sums: fold lane 16 into lane 0
+    for (int k = 0; k < D; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
 }
 

@@ -979,7 +979,18 @@ __global__ void __launch_bounds__(256) k_far_c(int first, int n_node, ProdArgs g
 // near field onto a leaf's points (one CTA per leaf, sources tiled through shared memory):
 //   near partner           : yp[i] += sum_{j != i} K(x_i, x_j) [1 | x_j]
 //   finer far partner (s)  : yp[i] += K(x_i, J_s) y0[s]
-template <int D>
+// NC = number of accumulated columns (3 in 2D for [1 | x y], 4 in 3D or for general inputs);
+// only the leaf's own tiles test for the diagonal.
+template <int NC>
+__device__ __forceinline__ void acc_cols(float4 &acc, float w, const float4 &v)
+{
+    acc.x = fmaf(w, v.x, acc.x);
+    acc.y = fmaf(w, v.y, acc.y);
+    acc.z = fmaf(w, v.z, acc.z);
+    if (NC == 4) acc.w = fmaf(w, v.w, acc.w);
+}
+
+template <int D, int NC>
 __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
 {
     constexpr int MAXR = Dim<D>::MAXR;
@@ -1008,10 +1019,16 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
                 }
                 __syncthreads();
                 const int lim = min(NEAR_THREADS, sc - tile);
-                for (int j = 0; j < lim; j++) {
-                    float w = rkernel(dist2(xi, sx[j]));
-                    w = (ss + tile + j == i) ? 0.f : w;
-                    fma4(acc, w, sxin[j]);
+                if (s == t) {
+                    const int self = i - (ss + tile);
+                    for (int j = 0; j < lim; j++) {
+                        float w = rkernel(dist2(xi, sx[j]));
+                        w = (j == self) ? 0.f : w;
+                        acc_cols<NC>(acc, w, sxin[j]);
+                    }
+                } else {
+#pragma unroll 4
+                    for (int j = 0; j < lim; j++) acc_cols<NC>(acc, rkernel(dist2(xi, sx[j])), sxin[j]);
                 }
             }
         }
@@ -1025,13 +1042,12 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
                 sy[b] = g.y0[(size_t)s * MAXR + b];
             }
             __syncthreads();
-            for (int b = 0; b < rs; b++) fma4(acc, rkernel(dist2(xi, sx[b])), sy[b]);
+            for (int b = 0; b < rs; b++) acc_cols<NC>(acc, rkernel(dist2(xi, sx[b])), sy[b]);
         }
         if (valid) g.yp[i] = acc;
     }
 }
 
-// downward pass, one warp per node of `level`: children's y1 / the leaf's points += U_t y1[t]
 // LEAVES = false: the internal nodes of `level` (run top-down); true: every leaf at level >= 2
 // (after all internal levels)
 template <int D, bool LEAVES>
@@ -1527,7 +1543,8 @@ private:
         k_far_c<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(first, n_node_, g);
         mark_end(t_far, 3);
         cudaEvent_t t_near = mark_begin();
-        k_near<D><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
+        if (D == 2 && xin == nullptr) k_near<D, 3><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
+        else k_near<D, 4><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
         mark_end(t_near, 4);
         launches_ += 2;
         cudaEvent_t t_down = mark_begin();

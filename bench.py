@@ -192,9 +192,8 @@ def ours(args, rank, world, local):
     dev_s = float(np.mean([r[1] for r in res]))
     wall_s = float(np.mean([r[0] for r in res]))
     if dist:
-        t = torch.tensor([dev_s, wall_s], device=f"cuda:{local}", dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        dev_s, wall_s = t.tolist()
+        from tsne_h2pack._replicas import max_over_ranks
+        dev_s, wall_s = max_over_ranks([dev_s, wall_s], device=f"cuda:{local}")
     attr_ms = sum(r[2] for r in res) / max(1, sum(r[3] for r in res))
     launches = int(sum(r[4] for r in res))
     kl = res[-1][6]

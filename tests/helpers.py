@@ -124,6 +124,17 @@ class Engine:
         Z = self.lib.compute_repulsive_forces_h2pack(h, Y, self.d, self.n, self.ws, grad, 0)
         return -grad, Z
 
+    def matmul(self, cols):
+        """W X of the workspace's H2 matrix for general columns (tsne_h2_matmul, diagonal
+        included), original point order; cols: sequence of length-n arrays."""
+        h = self.lib.tsne_get_h2_matrix(self.ws)
+        X = [np.ascontiguousarray(c, dtype=np.float64) for c in cols]
+        Yo = [np.zeros(self.n) for _ in X]
+        xp = (ctypes.c_void_p * len(X))(*[x.ctypes.data for x in X])
+        yp = (ctypes.c_void_p * len(X))(*[y.ctypes.data for y in Yo])
+        assert self.lib.tsne_h2_matmul(h, len(X), xp, yp, None) == 0
+        return np.array(Yo)
+
     def stats(self):
         nr = ctypes.c_int(); nl = ctypes.c_longlong()
         self.lib.tsne_get_run_stats(self.ws, ctypes.byref(nr), ctypes.byref(nl))

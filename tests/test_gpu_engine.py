@@ -8,6 +8,8 @@ iterations):
   - perplexity calibration vs the oracle: rtol 1e-10
   - H2 tree permutation, node table and near/far lists vs the oracle: bit-exact
   - H2 repulsive force vs the FP64 exact force: rel 2-norm <= h2_tol
+  - fused force product vs the general-column product of the same H2 matrix: rel 2e-5
+  - full schedule vs the oracle: embedding rel 1e-2 after 3 iterations, KL 0.5% after 29
   - attractive force vs the FP64 oracle: rel 1e-5
   - 1000-iteration run: KL within 1% of the oracle's run, 30-NN preservation within 0.5 points
 """
@@ -139,6 +141,25 @@ def test_h2_force_within_tolerance(mid, n_iter):
     assert abs(Z - Ze) <= 1e-2 * Ze
 
 
+@pytest.mark.parametrize("n_iter", [20, 300])
+def test_force_path_matches_general_product(mid, n_iter):
+    """The fused force product of the iteration ([1 | x y] columns, two target points per
+    thread) against the general-column product of the same H2 matrix (tsne_h2_matmul), from
+    which s, v, Z and the force follow by the reference's identities: both FP32, so they agree
+    to rounding (rel 2e-5)."""
+    X, G, P, _ = mid
+    Y = _evolved(P, n_iter, 2).astype(np.float32).astype(np.float64)
+    eng = Engine(P, Y, n_iter=1)
+    assert eng.rebuild() == 0
+    F, Z = eng.repulsive(Y)
+    W = eng.matmul([np.ones(Y.shape[1]), Y[0], Y[1]])
+    eng.close()
+    Zg, Fg = O.z_force(Y, W[0] - 1.0, W[1:] - Y)
+    print(f"iter {n_iter}: force rel {rel2(F, Fg):.3e}, Z rel {abs(Z - Zg) / Zg:.3e}")
+    assert rel2(F, Fg) < 2e-5
+    assert abs(Z - Zg) < 2e-5 * Zg
+
+
 def test_attractive_matches_oracle(mid):
     from tsne_h2pack._backend import scipy_csr_to_c_sparse_matrix
     X, G, P, _ = mid
@@ -156,7 +177,7 @@ def test_attractive_matches_oracle(mid):
 def test_short_trajectory_matches_oracle(mid):
     """Full schedule (H2 rebuild every iteration below 20). The device skeletons differ from
     the FP64 oracle's at the ID tolerance, a perturbation that t-SNE amplifies, so the
-    embeddings are compared after 3 iterations and the KL after 29."""
+    embeddings are compared after 3 iterations (rel 1e-2) and the KL after 29 (0.5%)."""
     X, G, P, _ = mid
     Y0 = O.init_embedding(P.shape[0], 2, 4)
     eng = Engine(P, Y0, n_iter=3)
@@ -168,7 +189,7 @@ def test_short_trajectory_matches_oracle(mid):
     Yo, klo = O.run(P, Y0, n_iter=29)
     print("3-iteration rel", r, "KL", eng.kl(), klo)
     assert r < 1e-2
-    assert abs(eng.kl() - klo) < 1e-3 * abs(klo)
+    assert abs(eng.kl() - klo) < 5e-3 * abs(klo)
 
 
 def test_renumbering_is_transparent(mid, monkeypatch):

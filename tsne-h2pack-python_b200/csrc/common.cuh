@@ -96,6 +96,58 @@ __device__ __forceinline__ float rkernel(float r2)
     return w * w;
 }
 
+// Packed pairs of floats for the sm_100 paired FP32 instructions (PTX add/sub/mul/fma .f32x2):
+// one instruction applies the operation to both halves, halving the issue slots of
+// arithmetic that runs on two independent lanes of data (here: two target points).
+struct F2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ F2 f2_pack(float lo, float hi)
+{
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(F2 a, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ F2 f2_sub(F2 a, F2 b)
+{
+    F2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 f2_add(F2 a, F2 b)
+{
+    F2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 f2_mul(F2 a, F2 b)
+{
+    F2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 f2_fma(F2 a, F2 b, F2 c)
+{
+    F2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+// (1 + |a - s|^2)^-2 for two targets a (packed x and y) against one source s (each
+// coordinate duplicated in both halves)
+__device__ __forceinline__ F2 f2_rkernel(F2 ax, F2 ay, F2 sx, F2 sy)
+{
+    const F2 dx = f2_sub(ax, sx), dy = f2_sub(ay, sy);
+    const F2 q = f2_fma(dx, dx, f2_fma(dy, dy, f2_pack(1.f, 1.f)));
+    float q0, q1;
+    f2_unpack(q, q0, q1);
+    const F2 w = f2_pack(fast_rcp(q0), fast_rcp(q1));
+    return f2_mul(w, w);
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v)
 {

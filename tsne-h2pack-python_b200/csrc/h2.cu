@@ -45,7 +45,11 @@ struct TreeView {
     int n, L, leaf_size, cap_node, nset_cap;
     const unsigned long long *keys;
     int *start, *end, *level, *parent, *fchild, *nchild, *leaf, *ix;
-    int *nch, *cb;
+    signed char *delta;      // shared leading digits with the previous key (n + 1)
+    int *fm;                 // per point: first | last level << 8 of the nodes it starts, or -1
+    int *blkcnt, *blkoff;    // per block of TREE_BLOCK points, 2 x 32 counts / offsets
+    int *bset, *nid;         // per level l: boundary starts B_l and their node ids (stride cap_node)
+    int *btot;               // |B_l|
     TreeInfo *info;
 };
 
@@ -178,105 +182,235 @@ __global__ void k_keys(int n, int L, const Vec<D> *__restrict__ Y, const TreeInf
     }
 }
 
+// ---------------------------------------------------------------------------------
+// tree: all levels at once from the sorted keys.
+//
+// delta[i] = number of leading base-2^D digits that key[i - 1] and key[i] share (L when equal;
+// -1 at i = 0 and at the sentinel i = n). A node of level l is a maximal run of points with
+// one l-digit prefix: it starts at a point s with delta[s] < l and ends at the next point
+// with delta < l. A node exists when its parent holds more than leaf_size points (and it is
+// at most at level L); the counts shrink down the tree, so that is the whole condition.
+//
+// Point s starts the nodes of levels f_s = delta[s] + 1 .. m_s when the node of level
+// delta[s] around it holds more than leaf_size points (E_s); m_s is the first level whose
+// node starting at s holds at most leaf_size points (the leaf), capped at L. Nodes are
+// numbered level by level in key order; the starts of level l's node boundaries,
+// B_l = {E points with f <= l}, give every node's end (the next entry of B_l), parent (the
+// entry of B_{l-1} at or before it) and children (the entries of B_{l+1} inside it).
+// ---------------------------------------------------------------------------------
+constexpr int TREE_BLOCK = 1024;   // points per block of the marking and numbering kernels
+
 template <int D>
-__global__ void k_gather(int n, const int *__restrict__ perm, const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ xt)
+__device__ __forceinline__ int shared_digits(unsigned long long a, unsigned long long b, int L)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) xt[i] = Y[perm[i]];
+    const unsigned long long x = a ^ b;
+    if (x == 0ULL) return L;
+    return (__clzll((long long)x) - (64 - D * L)) / D;
 }
 
-// ---------------------------------------------------------------------------------
-// tree levels: k_split finds the child ranges of the nodes of one level, k_emit (one
-// CTA) numbers the children in key order and writes them.
-// ---------------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(256) k_split(int l, TreeView tv)
+__device__ __forceinline__ unsigned int key_coord(unsigned long long key, int k, int L)
 {
-    constexpr int NCH = 1 << D;
-    if (tv.info->pad[0]) return;   // node capacity exceeded: the host regrows and rebuilds
-    const int lb = tv.info->level_begin[l], nl = min(tv.info->n_level_nodes[l], tv.cap_node);
-    const int shift = D * (tv.L - l - 1);
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
-        const int t = lb + j;
-        const int s = tv.start[t], e = tv.end[t];
-        int *cb = tv.cb + (size_t)j * (NCH + 1);
-        if (e - s <= tv.leaf_size || l >= tv.L) { tv.nch[j] = 0; continue; }
-        cb[0] = s;
-        cb[NCH] = e;
-        for (int c = 1; c < NCH; c++) {
-            int lo = s, hi = e;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (digit_of(tv.keys[mid], shift, NCH - 1) < c) lo = mid + 1; else hi = mid;
-            }
-            cb[c] = lo;
+    unsigned int q = 0;
+    for (int b = 0; b < L; b++) q |= (unsigned int)((key >> (D * b + k)) & 1ULL) << b;
+    return q;
+}
+
+// tree-order coordinates, and delta (with its sentinel)
+template <int D>
+__global__ void k_gather(int n, int L, const int *__restrict__ perm, const Vec<D> *__restrict__ Y,
+                         Vec<D> *__restrict__ xt, const unsigned long long *__restrict__ keys,
+                         signed char *__restrict__ delta)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+        if (i == n) {
+            delta[n] = -1;
+            continue;
         }
-        int cnt = 0;
-        for (int c = 0; c < NCH; c++) cnt += cb[c + 1] > cb[c];
-        tv.nch[j] = cnt;
+        xt[i] = Y[perm[i]];
+        delta[i] = i == 0 ? (signed char)-1 : (signed char)shared_digits<D>(keys[i - 1], keys[i], L);
     }
 }
 
-template <int D>
-__global__ void __launch_bounds__(1024) k_emit(int l, TreeView tv)
+// per point: E, f, m packed in fm (-1: starts no node); per block and level the number of
+// node starts and of boundary starts
+__device__ __forceinline__ void tree_bits(int fm, int l, bool &bn, bool &bb)
 {
-    constexpr int NCH = 1 << D;
-    using Scan = cub::BlockScan<int, 1024>;
-    __shared__ typename Scan::TempStorage tmp;
-    __shared__ int s_run;
+    const int f = fm & 0xff, m = fm >> 8;
+    bb = fm >= 0 && f <= l;
+    bn = bb && l <= m;
+}
+
+template <int D>
+__global__ void __launch_bounds__(TREE_BLOCK) k_tree_marks(TreeView tv)
+{
+    __shared__ int wc[2][32][TREE_BLOCK / 32];
+    const int n = tv.n, L = tv.L, leaf = tv.leaf_size;
+    const signed char *delta = tv.delta;
+    const int s = blockIdx.x * TREE_BLOCK + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int fm = -1;
+    if (s < n) {
+        const int ds = delta[s], f = ds + 1;
+        bool E = s == 0;
+        if (s > 0) {
+            int j = s - 1;
+            while (delta[j] >= ds && s - j <= leaf) j--;   // delta[0] = -1 ends the walk
+            const int left = s - j;
+            if (left > leaf) E = true;
+            else {
+                int k = s + 1;
+                while (k < n && delta[k] >= ds && left + (k - s) <= leaf) k++;
+                E = left + (k - s) > leaf;
+            }
+        }
+        if (f > L) E = false;
+        if (E) {
+            int mu = L + 1;
+            const int last = min(s + leaf, n);
+            for (int j = s + 1; j <= last && mu >= f; j++) mu = min(mu, (int)delta[j]);
+            const int m = min(L, max(f, mu + 1));
+            fm = f | (m << 8);
+        }
+        tv.fm[s] = fm;
+    }
+    for (int l = 0; l <= L; l++) {
+        bool bn, bb;
+        tree_bits(fm, l, bn, bb);
+        const unsigned vn = __ballot_sync(0xffffffffu, bn), vb = __ballot_sync(0xffffffffu, bb);
+        if (lane == 0) { wc[0][l][w] = __popc(vn); wc[1][l][w] = __popc(vb); }
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        const int arr = threadIdx.x >> 5, l = threadIdx.x & 31;
+        int c = 0;
+        if (l <= L)
+            for (int k = 0; k < TREE_BLOCK / 32; k++) c += wc[arr][l][k];
+        tv.blkcnt[((size_t)blockIdx.x * 2 + arr) * 32 + l] = c;
+    }
+}
+
+// one CTA: block offsets per level (exclusive scans over the blocks), level table, totals
+__global__ void __launch_bounds__(1024) k_tree_scan(int nblk, TreeView tv)
+{
+    __shared__ int tot[2][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int col = w; col < 64; col += 32) {
+        int run = 0;
+        for (int b0 = 0; b0 < nblk; b0 += 32) {
+            const int b = b0 + lane;
+            const size_t at = ((size_t)b * 2 + (col >> 5)) * 32 + (col & 31);
+            const int v = b < nblk ? tv.blkcnt[at] : 0;
+            int x = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (b < nblk) tv.blkoff[at] = run + x - v;
+            run += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) tot[col >> 5][col & 31] = run;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        TreeInfo *info = tv.info;
+        int acc = 0, maxl = 0;
+        for (int l = 0; l < 32; l++) {
+            const int c = l <= tv.L ? tot[0][l] : 0;
+            info->level_begin[l] = acc;
+            info->n_level_nodes[l] = c;
+            if (c > 0) maxl = l;
+            acc += c;
+            tv.btot[l] = l <= tv.L ? tot[1][l] : 0;
+        }
+        info->level_begin[32] = acc;
+        info->n_node = acc;
+        info->max_level = maxl;
+        if (acc > tv.cap_node) info->pad[0] = 1;
+    }
+}
+
+// numbers the nodes and writes their start, level, leaf flag, box index and first child;
+// end, parent and child count are stored as positions in the boundary lists for k_tree_finish
+template <int D>
+__global__ void __launch_bounds__(TREE_BLOCK) k_tree_emit(TreeView tv)
+{
+    __shared__ int wo[2][32][TREE_BLOCK / 32];
+    const TreeInfo *info = tv.info;
+    if (info->pad[0]) return;
+    const int n = tv.n, L = tv.L;
+    const int s = blockIdx.x * TREE_BLOCK + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int fm = s < n ? tv.fm[s] : -1;
+    for (int l = 0; l <= L; l++) {
+        bool bn, bb;
+        tree_bits(fm, l, bn, bb);
+        const unsigned vn = __ballot_sync(0xffffffffu, bn), vb = __ballot_sync(0xffffffffu, bb);
+        if (lane == 0) { wo[0][l][w] = __popc(vn); wo[1][l][w] = __popc(vb); }
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {   // exclusive scan over the warps, per array and level
+        const int arr = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l <= L) {
+            int run = 0;
+            for (int k = 0; k < TREE_BLOCK / 32; k++) { const int c = wo[arr][l][k]; wo[arr][l][k] = run; run += c; }
+        }
+    }
+    __syncthreads();
+    const size_t cap = (size_t)tv.cap_node;
+    const unsigned long long key = s < n ? tv.keys[s] : 0ULL;
+    const int f = fm & 0xff, m = fm >> 8;
+    int prev_br = 0, prev_id = -1;
+    for (int l = 0; l <= L; l++) {
+        bool bn, bb;
+        tree_bits(fm, l, bn, bb);
+        const unsigned vn = __ballot_sync(0xffffffffu, bn), vb = __ballot_sync(0xffffffffu, bb);
+        const int br = tv.blkoff[((size_t)blockIdx.x * 2 + 1) * 32 + l] + wo[1][l][w] + __popc(vb & lt);
+        if (bb) {
+            int id = -1;
+            if (bn) {
+                const int nr = tv.blkoff[((size_t)blockIdx.x * 2 + 0) * 32 + l] + wo[0][l][w] + __popc(vn & lt);
+                id = info->level_begin[l] + nr;
+                tv.start[id] = s;
+                tv.level[id] = l;
+                tv.leaf[id] = l == m ? 1 : 0;
+                for (int k = 0; k < 3; k++)
+                    tv.ix[(size_t)id * 3 + k] = k < D ? (int)(key_coord<D>(key, k, L) >> (L - l)) : 0;
+                tv.end[id] = br;
+                tv.parent[id] = l == 0 ? -1 : (f <= l - 1 ? prev_br : prev_br - 1);
+                tv.fchild[id] = -1;
+                tv.nchild[id] = 0;
+                if (prev_id >= 0) { tv.fchild[prev_id] = id; tv.nchild[prev_id] = br; }
+            }
+            tv.bset[(size_t)l * cap + br] = s;
+            tv.nid[(size_t)l * cap + br] = id;
+            prev_id = id;
+        }
+        prev_br = br;
+    }
+}
+
+// end, parent and child count of every node from the boundary lists; the largest leaf
+template <int D>
+__global__ void k_tree_finish(TreeView tv)
+{
     TreeInfo *info = tv.info;
     if (info->pad[0]) return;
-    const int lb = info->level_begin[l], nl = min(info->n_level_nodes[l], tv.cap_node);
-    const int next = lb + nl;
-    if (threadIdx.x == 0) s_run = 0;
-    __syncthreads();
-    for (int chunk = 0; chunk < nl; chunk += 1024) {
-        const int j = chunk + threadIdx.x;
-        const int x = j < nl ? tv.nch[j] : 0;
-        int off, total;
-        Scan(tmp).ExclusiveSum(x, off, total);
-        const int run = s_run;
-        if (j < nl) {
-            const int t = lb + j;
-            int ml = 0;
-            if (x > 0) {
-                int child = next + run + off;
-                tv.fchild[t] = child;
-                tv.nchild[t] = x;
-                tv.leaf[t] = 0;
-                const int *cb = tv.cb + (size_t)j * (NCH + 1);
-                for (int c = 0; c < NCH; c++) {
-                    const int s = cb[c], e = cb[c + 1];
-                    if (e <= s) continue;
-                    if (child < tv.cap_node) {
-                        tv.start[child] = s; tv.end[child] = e; tv.level[child] = l + 1; tv.parent[child] = t;
-                        tv.fchild[child] = -1; tv.nchild[child] = 0; tv.leaf[child] = 1;
-                        for (int k = 0; k < 3; k++)
-                            tv.ix[(size_t)child * 3 + k] = k < D ? 2 * tv.ix[(size_t)t * 3 + k] + ((c >> k) & 1) : 0;
-                    } else {
-                        atomicExch(&info->pad[0], 1);
-                    }
-                    child++;
-                }
-            } else {
-                tv.fchild[t] = -1;
-                tv.nchild[t] = 0;
-                tv.leaf[t] = 1;
-                ml = tv.end[t] - tv.start[t];
-            }
-            if (ml > 0) atomicMax(&info->max_leaf, ml);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) s_run = run + total;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const int run = s_run;
-        info->level_begin[l + 1] = next;
-        if (l + 1 < 32) info->n_level_nodes[l + 1] = run;
-        info->level_begin[l + 2 < 33 ? l + 2 : 32] = next + run;
-        if (nl > 0) {
-            info->max_level = run > 0 ? l + 1 : l;
-            info->n_node = next + run;
+    const int n_node = info->n_node;
+    const size_t cap = (size_t)tv.cap_node;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x) {
+        const int l = tv.level[t], s = tv.start[t], pos = tv.end[t];
+        const int e = pos + 1 < tv.btot[l] ? tv.bset[(size_t)l * cap + pos + 1] : tv.n;
+        tv.end[t] = e;
+        if (l > 0) tv.parent[t] = tv.nid[(size_t)(l - 1) * cap + tv.parent[t]];
+        if (tv.leaf[t]) {
+            atomicMax(&info->max_leaf, e - s);
+        } else {
+            const int c0 = tv.nchild[t], lim = tv.btot[l + 1];
+            int c = 0;
+            while (c0 + c < lim && tv.bset[(size_t)(l + 1) * cap + c0 + c] < e) c++;
+            tv.nchild[t] = c;
         }
     }
 }
@@ -1048,6 +1182,102 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
     }
 }
 
+// Near field of the 2D force product ([1 | x y] columns), two targets per thread with the
+// paired FP32 instructions: thread `tid` owns the leaf's points tid and tid + NEAR2_THREADS of
+// each chunk of 2 * NEAR2_THREADS. Sources are staged with each coordinate duplicated
+// ((x, x), (y, y)), so one shared-memory load feeds both targets; per source and target pair
+// the kernel issues 5 arithmetic instructions and 2 reciprocals instead of 10 and 2.
+// Same sums, same order of sources, as k_near.
+constexpr int NEAR2_THREADS = 64;
+constexpr int NEAR2_TILE = 2 * NEAR2_THREADS;
+
+__global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
+{
+    constexpr int MAXR = Dim<2>::MAXR;
+    const TreeView &tv = g.tv;
+    const int t = blockIdx.x;
+    if (!tv.leaf[t]) return;
+    const float2 *xt = (const float2 *)g.xt;
+    const float2 *skel = (const float2 *)g.skel;
+    __shared__ float4 sxy[NEAR2_TILE];      // (x, x, y, y)
+    __shared__ float4 sw01[MAXR];           // (w0, w0, w1, w1) of a skeleton source
+    __shared__ float2 sw2[MAXR];            // (w2, w2)
+    const int tid = threadIdx.x;
+    const int s0 = tv.start[t], cnt = tv.end[t] - s0, lt = tv.level[t];
+    for (int chunk = 0; chunk < cnt; chunk += NEAR2_TILE) {
+        const int a0 = chunk + tid, a1 = a0 + NEAR2_THREADS;
+        const float2 x0 = xt[s0 + (a0 < cnt ? a0 : 0)], x1 = xt[s0 + (a1 < cnt ? a1 : 0)];
+        const F2 ax = f2_pack(x0.x, x1.x), ay = f2_pack(x0.y, x1.y);
+        F2 acc0 = f2_pack(0.f, 0.f), accx = acc0, accy = acc0;
+        for (int e = g.near_ptr[t]; e < g.near_ptr[t + 1]; e++) {
+            const int s = g.near_idx[e];
+            const int ss = tv.start[s], sc = tv.end[s] - ss;
+            for (int tile = 0; tile < sc; tile += NEAR2_TILE) {
+                __syncthreads();
+                for (int b = tid; b < NEAR2_TILE && b < sc - tile; b += NEAR2_THREADS) {
+                    const float2 p = xt[ss + tile + b];
+                    sxy[b] = make_float4(p.x, p.x, p.y, p.y);
+                }
+                __syncthreads();
+                const int lim = min(NEAR2_TILE, sc - tile);
+                if (s == t) {
+                    const int self0 = a0 - tile, self1 = a1 - tile;
+                    for (int j = 0; j < lim; j++) {
+                        const float4 q = sxy[j];
+                        const F2 sx = f2_pack(q.x, q.y), sy = f2_pack(q.z, q.w);
+                        F2 w = f2_rkernel(ax, ay, sx, sy);
+                        float w0, w1;
+                        f2_unpack(w, w0, w1);
+                        w = f2_pack(j == self0 ? 0.f : w0, j == self1 ? 0.f : w1);
+                        acc0 = f2_add(acc0, w);
+                        accx = f2_fma(w, sx, accx);
+                        accy = f2_fma(w, sy, accy);
+                    }
+                } else {
+#pragma unroll 4
+                    for (int j = 0; j < lim; j++) {
+                        const float4 q = sxy[j];
+                        const F2 sx = f2_pack(q.x, q.y), sy = f2_pack(q.z, q.w);
+                        const F2 w = f2_rkernel(ax, ay, sx, sy);
+                        acc0 = f2_add(acc0, w);
+                        accx = f2_fma(w, sx, accx);
+                        accy = f2_fma(w, sy, accy);
+                    }
+                }
+            }
+        }
+        for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++) {
+            const int s = g.far_idx[e];
+            if (tv.level[s] <= lt) continue;
+            const int rs = g.rank[s];
+            __syncthreads();
+            for (int b = tid; b < rs; b += NEAR2_THREADS) {
+                const float2 p = skel[(size_t)s * MAXR + b];
+                const float4 y = g.y0[(size_t)s * MAXR + b];
+                sxy[b] = make_float4(p.x, p.x, p.y, p.y);
+                sw01[b] = make_float4(y.x, y.x, y.y, y.y);
+                sw2[b] = make_float2(y.z, y.z);
+            }
+            __syncthreads();
+            for (int b = 0; b < rs; b++) {
+                const float4 q = sxy[b];
+                const float4 y01 = sw01[b];
+                const float2 y2 = sw2[b];
+                const F2 w = f2_rkernel(ax, ay, f2_pack(q.x, q.y), f2_pack(q.z, q.w));
+                acc0 = f2_fma(w, f2_pack(y01.x, y01.y), acc0);
+                accx = f2_fma(w, f2_pack(y01.z, y01.w), accx);
+                accy = f2_fma(w, f2_pack(y2.x, y2.y), accy);
+            }
+        }
+        float c00, c01, cx0, cx1, cy0, cy1;
+        f2_unpack(acc0, c00, c01);
+        f2_unpack(accx, cx0, cx1);
+        f2_unpack(accy, cy0, cy1);
+        if (a0 < cnt) g.yp[s0 + a0] = make_float4(c00, cx0, cy0, 0.f);
+        if (a1 < cnt) g.yp[s0 + a1] = make_float4(c01, cx1, cy1, 0.f);
+    }
+}
+
 // LEAVES = false: the internal nodes of `level` (run top-down); true: every leaf at level >= 2
 // (after all internal levels)
 template <int D, bool LEAVES>
@@ -1131,6 +1361,11 @@ public:
         keys_in_.exact(n); keys_.exact(n); idx_in_.exact(n); perm_.exact(n); xt_.exact(n);
         yp_.exact(n); s_.exact(n); v_.exact(n);
         bbox_part_.exact((size_t)BBOX_BLOCKS * (2 * D + 1));
+        delta_.exact((size_t)n + 1);
+        fm_.exact(n);
+        blkcnt_.exact((size_t)ceil_div(n, TREE_BLOCK) * 64);
+        blkoff_.exact((size_t)ceil_div(n, TREE_BLOCK) * 64);
+        btot_.exact(32);
         info_.exact(1);
         size_t b1 = 0, b2 = 0;
         TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, b1, keys_in_.p, keys_.p, idx_in_.p,
@@ -1154,31 +1389,33 @@ public:
         const int L = Dim<D>::L;
         cudaEvent_t t_tree = mark_begin();
         sec_begin();
-        // One batch: root box, keys, sort, tree levels and the counting pass of the interaction
-        // lists (kernels read the level and node counts on the device; scans run over the node
-        // capacity, whose unused tail counts are zero), then a single synchronisation reads the
-        // tree, the list totals and the basis rows. A deeper tree than the launched levels, a
-        // full node table or a full inadmissible-source set are caught there and redone.
-        int launched = 0;
+        // One batch: root box, keys, sort, the whole tree (four kernels over the points, no level
+        // loop) and the counting pass of the interaction lists (kernels read the level and node
+        // counts on the device; scans run over the node capacity, whose unused tail counts are
+        // zero), then a single synchronisation reads the tree, the list totals and the basis
+        // rows. A full node table, a tree deeper than the list levels counted or a full
+        // inadmissible-source set are caught there and redone.
+        bool tree_ok = false;
+        int list_levels = std::min(L + 1, std::max(6, last_max_level_ + 2));
         for (int attempt = 0; attempt < 12; attempt++) {
-            if (launched == 0) {
+            if (!tree_ok) {
+                const int nblk = ceil_div(n_, TREE_BLOCK);
                 k_bbox<D><<<BBOX_BLOCKS, 256, 0, st_>>>(n_, (const Vec<D> *)Y, bbox_part_.p);
                 k_root<D><<<1, 256, 0, st_>>>(n_, L, BBOX_BLOCKS, bbox_part_.p, view());
                 k_keys<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, L, (const Vec<D> *)Y, info_.p, keys_in_.p, idx_in_.p);
                 size_t bytes = sort_bytes_;
                 TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, bytes, keys_in_.p, keys_.p, idx_in_.p,
                                                                 perm_.p, n_, 0, D * L, st_));
-                k_gather<D><<<grid_for(n_, 256), 256, 0, st_>>>(n_, perm_.p, (const Vec<D> *)Y, (Vec<D> *)xt_.p);
-                launches_ += 5 + 4;
+                k_gather<D><<<grid_for(n_ + 1, 256), 256, 0, st_>>>(n_, L, perm_.p, (const Vec<D> *)Y,
+                                                                     (Vec<D> *)xt_.p, keys_.p, delta_.p);
+                k_tree_marks<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());
+                k_tree_scan<<<1, 1024, 0, st_>>>(nblk, view());
+                k_tree_emit<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());
+                k_tree_finish<D><<<grid_for(cap_node_, 256, 148 * 8), 256, 0, st_>>>(view());
+                launches_ += 9 + 4;
+                tree_ok = true;
             }
-            const int want = std::min(L + 1, std::max(launched + 4, std::max(6, last_max_level_ + 2)));
-            for (int l = launched; l < want; l++) {
-                k_split<D><<<148, 256, 0, st_>>>(l, view());
-                k_emit<D><<<1, 1024, 0, st_>>>(l, view());
-                launches_ += 2;
-            }
-            launched = want;
-            launch_list_counts(want);
+            launch_list_counts(list_levels);
             TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
@@ -1189,20 +1426,17 @@ public:
             if (I.pad[0]) {   // node table full: grow and start over
                 cap_node_ *= 2;
                 alloc_nodes();
-                launched = 0;
+                tree_ok = false;
                 continue;
             }
-            if (launched <= L && launched < 31 && I.n_level_nodes[launched] > 0) continue;   // deeper tree
+            if (list_levels < I.max_level) {   // internal targets below the counted levels
+                list_levels = std::min(L + 1, I.max_level + 1);
+                continue;
+            }
             if (I.nset_overflow) {   // inadmissible-source set full: grow, recount
                 nset_cap_ *= 2;
                 alloc_lists();
-                launch_list_counts(launched);
-                TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
-                TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
-                TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
-                TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + cap_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
-                TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
-                if (hinfo_.p->nset_overflow && attempt < 11) continue;
+                if (attempt < 11) continue;
             }
             break;
         }
@@ -1477,8 +1711,9 @@ private:
     {
         const size_t c = cap_node_;
         start_.exact(c); end_.exact(c); level_.exact(c); parent_.exact(c); fchild_.exact(c);
-        nchild_.exact(c); leaf_.exact(c); ix_.exact(3 * c); nch_.exact(c);
-        cb_.exact(c * ((1 << D) + 1));
+        nchild_.exact(c); leaf_.exact(c); ix_.exact(3 * c);
+        bset_.exact(c * (Dim<D>::L + 1));
+        nid_.exact(c * (Dim<D>::L + 1));
         alloc_lists();
     }
 
@@ -1487,8 +1722,9 @@ private:
         TreeView v;
         v.n = n_; v.L = Dim<D>::L; v.leaf_size = leaf_size_; v.cap_node = cap_node_; v.nset_cap = nset_cap_;
         v.keys = keys_.p; v.start = start_.p; v.end = end_.p; v.level = level_.p; v.parent = parent_.p;
-        v.fchild = fchild_.p; v.nchild = nchild_.p; v.leaf = leaf_.p; v.ix = ix_.p; v.nch = nch_.p;
-        v.cb = cb_.p; v.info = info_.p;
+        v.fchild = fchild_.p; v.nchild = nchild_.p; v.leaf = leaf_.p; v.ix = ix_.p;
+        v.delta = delta_.p; v.fm = fm_.p; v.blkcnt = blkcnt_.p; v.blkoff = blkoff_.p;
+        v.bset = bset_.p; v.nid = nid_.p; v.btot = btot_.p; v.info = info_.p;
         return v;
     }
 
@@ -1543,7 +1779,7 @@ private:
         k_far_c<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(first, n_node_, g);
         mark_end(t_far, 3);
         cudaEvent_t t_near = mark_begin();
-        if (D == 2 && xin == nullptr) k_near<D, 3><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
+        if (D == 2 && xin == nullptr) k_near2d<<<n_node_, NEAR2_THREADS, 0, st_>>>(g);
         else k_near<D, 4><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
         mark_end(t_near, 4);
         launches_ += 2;
@@ -1578,7 +1814,9 @@ private:
     DevBuf<double> bbox_part_;
     DevBuf<TreeInfo> info_;
     HostPinned<TreeInfo> hinfo_;
-    DevBuf<int> start_, end_, level_, parent_, fchild_, nchild_, leaf_, ix_, nch_, cb_;
+    DevBuf<int> start_, end_, level_, parent_, fchild_, nchild_, leaf_, ix_;
+    DevBuf<signed char> delta_;
+    DevBuf<int> fm_, blkcnt_, blkoff_, bset_, nid_, btot_;
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;
     DevBuf<int> rowcap_;
     DevBuf<long long> rowoff_;

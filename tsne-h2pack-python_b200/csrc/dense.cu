@@ -438,45 +438,26 @@ __global__ void k_row_len(int n, const int *__restrict__ ord, const int *__restr
 }
 
 // Renumbered rows (reference tsne_reorder.c:112-167): new row k is old row ord[k] with its
-// columns mapped through inv. Emits, for the first transpose, key = new column and value =
-// (new row << 32 | value bits), entries grouped by new row in increasing order.
-__global__ void k_row_copy(int n, const int *__restrict__ ord, const int *__restrict__ inv,
-                           const int *__restrict__ rp_old, const int *__restrict__ col_old,
-                           const float *__restrict__ val_old, const int *__restrict__ rp_new,
-                           unsigned int *__restrict__ key, unsigned long long *__restrict__ pack)
+// columns mapped through inv, one warp per row, four entries per lane (rows are padded to
+// multiples of 4, so every row starts on a 16-byte boundary). The entries keep their order
+// inside the row.
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_row_gather(int n, const int *__restrict__ ord, const int *__restrict__ inv, const int *__restrict__ rp_old,
+             const int *__restrict__ col_old, const float *__restrict__ val_old, const int *__restrict__ rp_new,
+             int *__restrict__ col_new, float *__restrict__ val_new)
 {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarp = (gridDim.x * blockDim.x) >> 5;
     for (int k = warp; k < n; k += nwarp) {
         const int i = ord[k], b = rp_old[i], len = rp_old[i + 1] - b, o = rp_new[k];
-        for (int e = lane; e < len; e += 32) {
-            key[o + e] = (unsigned int)inv[col_old[b + e]];
-            pack[o + e] = ((unsigned long long)(unsigned int)k << 32) | __float_as_uint(val_old[b + e]);
+        for (int e = 4 * lane; e < len; e += 128) {
+            int4 c = ld_stream_i4(col_old + b + e);
+            const float4 v = ld_stream_f4(val_old + b + e);
+            c.x = inv[c.x]; c.y = inv[c.y]; c.z = inv[c.z]; c.w = inv[c.w];
+            *reinterpret_cast<int4 *>(col_new + o + e) = c;
+            *reinterpret_cast<float4 *>(val_new + o + e) = v;
         }
-    }
-}
-
-// After the first (stable) sort by new column c: key = new row, value = (c << 32 | bits)
-__global__ void k_swap_pack(long long nnz, const unsigned int *__restrict__ key_in,
-                            const unsigned long long *__restrict__ pack_in, unsigned int *__restrict__ key_out,
-                            unsigned long long *__restrict__ pack_out)
-{
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
-        const unsigned long long p = pack_in[e];
-        key_out[e] = (unsigned int)(p >> 32);
-        pack_out[e] = ((unsigned long long)key_in[e] << 32) | (p & 0xffffffffull);
-    }
-}
-
-// After the second sort by new row: entries are grouped by row and sorted by column
-__global__ void k_unpack(long long nnz, const unsigned long long *__restrict__ pack, int *__restrict__ col,
-                         float *__restrict__ val)
-{
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
-        const unsigned long long p = pack[e];
-        col[e] = (int)(p >> 32);
-        val[e] = __uint_as_float((unsigned int)(p & 0xffffffffull));
     }
 }
 
@@ -623,22 +604,10 @@ void launch_row_len(cudaStream_t st, int n, const int *ord, const int *rp_old, i
     k_row_len<<<ew_grid(n), EW_BLOCK, 0, st>>>(n, ord, rp_old, len_new);
 }
 
-void launch_row_copy(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
-                     const int *col_old, const float *val_old, const int *rp_new, unsigned int *key,
-                     unsigned long long *pack)
+void launch_row_gather(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
+                       const int *col_old, const float *val_old, const int *rp_new, int *col_new, float *val_new)
 {
-    k_row_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, ord, inv, rp_old, col_old, val_old, rp_new, key, pack);
-}
-
-void launch_swap_pack(cudaStream_t st, long long nnz, const unsigned int *key_in, const unsigned long long *pack_in,
-                      unsigned int *key_out, unsigned long long *pack_out)
-{
-    k_swap_pack<<<148 * 16, 256, 0, st>>>(nnz, key_in, pack_in, key_out, pack_out);
-}
-
-void launch_unpack(cudaStream_t st, long long nnz, const unsigned long long *pack, int *col, float *val)
-{
-    k_unpack<<<148 * 16, 256, 0, st>>>(nnz, pack, col, val);
+    k_row_gather<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, ord, inv, rp_old, col_old, val_old, rp_new, col_new, val_new);
 }
 
 void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist, double perplexity,

@@ -91,8 +91,6 @@ struct tsne_workspace {
 
     cudaStream_t st = nullptr;
     DevBuf<int> rp, col, rp2, col2, len, inv, order, order2;
-    DevBuf<unsigned int> rkey[2];              // renumbering: sort keys
-    DevBuf<unsigned long long> rpack[2];       // renumbering: (index, value) pairs
     long long padded_nnz = 0;
     DevBuf<float> val, val2;
     DevBuf<unsigned char> Y, Yn, uY, gains, rep, frc, tmpv, Yconv;
@@ -224,11 +222,11 @@ int rebuild_h2(tsne_workspace *ws)
     return 0;
 }
 
-// Renumbering (reference tsne_reorder.c:112-167): new point k = old point ord[k]. P is
-// renumbered like the reference does it, by two transposes whose stable ordering leaves every
-// row sorted by its new column: entries are emitted in new-row order with key = new column,
-// stably radix-sorted (grouping them by column, rows ascending inside a group), re-keyed by
-// row and sorted again. Then every per-point array is permuted and the cumulative order
+// Renumbering (reference tsne_reorder.c:112-167): new point k = old point ord[k]. New row k
+// of P is old row ord[k] with its columns mapped through the inverse permutation, in one
+// gather pass (the reference transposes twice, which also sorts every row by its new column;
+// the entries of a row are the same here, in their previous order, so the attractive sums
+// differ only in rounding). Then every per-point array is permuted and the cumulative order
 // updated. No host synchronisation.
 template <int D>
 void renumber_impl(tsne_workspace *ws, const int *ord_dev)
@@ -247,28 +245,9 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     ws->cub_tmp.ensure(bytes + 256);
     bytes = ws->cub_tmp.cap;
     TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(ws->cub_tmp.p, bytes, ws->len.p, ws->rp2.p + 1, n, st));
-    ws->rkey[0].exact(nnz); ws->rkey[1].exact(nnz);
-    ws->rpack[0].exact(nnz); ws->rpack[1].exact(nnz);
-    launch_row_copy(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, ws->rkey[0].p,
-                    ws->rpack[0].p);
-    int bits = 1;
-    while ((1LL << bits) < n) bits++;
-    size_t sb = 0;
-    TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, sb, ws->rkey[0].p, ws->rkey[1].p, ws->rpack[0].p,
-                                                    ws->rpack[1].p, nnz, 0, bits, st));
-    ws->cub_tmp.ensure(sb + 256);
-    sb = ws->cub_tmp.cap;
-    // first transpose: group by new column (rows stay ascending: the sort is stable)
-    TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(ws->cub_tmp.p, sb, ws->rkey[0].p, ws->rkey[1].p, ws->rpack[0].p,
-                                                    ws->rpack[1].p, nnz, 0, bits, st));
-    launch_swap_pack(st, nnz, ws->rkey[1].p, ws->rpack[1].p, ws->rkey[0].p, ws->rpack[0].p);
-    // second transpose: group by new row, columns ascending
-    sb = ws->cub_tmp.cap;
-    TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(ws->cub_tmp.p, sb, ws->rkey[0].p, ws->rkey[1].p, ws->rpack[0].p,
-                                                    ws->rpack[1].p, nnz, 0, bits, st));
     ws->col2.exact(std::max<long long>(nnz, 4));
     ws->val2.exact(std::max<long long>(nnz, 4));
-    launch_unpack(st, nnz, ws->rpack[1].p, ws->col2.p, ws->val2.p);
+    launch_row_gather(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, ws->col2.p, ws->val2.p);
     std::swap(ws->rp.p, ws->rp2.p); std::swap(ws->rp.cap, ws->rp2.cap);
     std::swap(ws->col.p, ws->col2.p); std::swap(ws->col.cap, ws->col2.cap);
     std::swap(ws->val.p, ws->val2.p); std::swap(ws->val.cap, ws->val2.cap);
@@ -285,7 +264,7 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     std::swap(ws->order.p, ws->order2.p);
     std::swap(ws->order.cap, ws->order2.cap);
     ws->has_order = true;
-    ws->n_launch += 16;
+    ws->n_launch += 11;
 }
 
 void renumber(tsne_workspace *ws, const int *ord_dev)

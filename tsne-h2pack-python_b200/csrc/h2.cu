@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cstdio>
 #include <cstdlib>
 #include <vector>
 
@@ -537,17 +538,31 @@ __global__ void __launch_bounds__(128) k_lists_write(int n_node, TreeView tv, Li
 
 // rows of each node's interpolation matrix: a leaf's points, or (upper bound) the
 // children's skeletons; nodes above MIN_ADM_LEVEL are not compressed
+// iflag / lflag: 1 for the internal nodes / leaves at level >= MIN_ADM_LEVEL (the items of
+// the basis launches)
 template <int D>
-__global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap)
+__global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap, int *__restrict__ iflag, int *__restrict__ lflag)
 {
     constexpr int NCH = 1 << D;
     const int n_node = tv.info->n_node;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x) {
         int r = 0;
-        if (tv.level[t] >= MIN_ADM_LEVEL) r = tv.leaf[t] ? tv.end[t] - tv.start[t] : NCH * Dim<D>::MAXR;
+        const bool adm = tv.level[t] >= MIN_ADM_LEVEL;
+        if (adm) r = tv.leaf[t] ? tv.end[t] - tv.start[t] : NCH * Dim<D>::MAXR;
         rowcap[t] = r;
+        iflag[t] = adm && !tv.leaf[t];
+        lflag[t] = adm && tv.leaf[t];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) rowcap[n_node] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { rowcap[n_node] = 0; iflag[n_node] = 0; lflag[n_node] = 0; }
+}
+
+// ids of the flagged nodes in increasing order
+__global__ void k_flag_list(const int *__restrict__ n_node_p, const int *__restrict__ flag,
+                            const int *__restrict__ pos, int *__restrict__ list)
+{
+    const int n_node = *n_node_p;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x)
+        if (flag[t]) list[pos[t]] = t;
 }
 
 // ---------------------------------------------------------------------------------
@@ -794,140 +809,243 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     }
 }
 
-// Register-resident ID (2D): thread `tid` owns candidate rows tid + ID_THREADS * j (j < RPT),
-// each a row of A = K(candidate - c, proxies) held in registers; the pivot row of a step is
-// normalised by its owner and broadcast through shared memory. Per step every thread
-// projects the pivot out of its rows, refreshes their norms, records the dot products in
-// the node's U rows (R12) and proposes its best remaining row; two barriers per step.
-// The column of R11 produced by a step goes to shared memory. Same decomposition, same
-// stopping rule and same U layout as k_id.
-template <bool LEAVES, int RPT>
-__global__ void __launch_bounds__(ID_THREADS, RPT == 1 ? 4 : 2) k_id_reg(int level, IdArgs g)
+__device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
 {
-    constexpr int P = Dim<2>::NPROXY, MAXR = Dim<2>::MAXR, NW = ID_THREADS / 32;
-    using V2 = float2;
-    const TreeView &tv = g.tv;
-    const int t = tv.info->level_begin[LEAVES ? MIN_ADM_LEVEL : level] + blockIdx.x;
-    if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) return;
-    const int lvl = tv.level[t];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const V2 *xt = (const V2 *)g.xt;
-    V2 *skel = (V2 *)g.skel;
+    acc.x = fmaf(w, v.x, acc.x); acc.y = fmaf(w, v.y, acc.y);
+    acc.z = fmaf(w, v.z, acc.z); acc.w = fmaf(w, v.w, acc.w);
+}
+__device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
 
+// ---------------------------------------------------------------------------------
+// dependency-ordered launches
+//
+// A kernel that processes the nodes of several levels in one launch takes its work items from
+// a ticket counter, so items start in ticket order whatever order the hardware dispatches
+// blocks in. An item waits only for items with smaller tickets, which are held by running
+// blocks or finished, so every wait ends. The waits are bounded all the same: after
+// DEP_WAIT_LIMIT polls the waiting thread records the failure (the host reports it) and goes on.
+// ---------------------------------------------------------------------------------
+constexpr int DEP_WAIT_LIMIT = 1 << 22;
+
+struct DepArgs {
+    int *flag;      // per node: epoch of the last launch that finished it
+    int *ticket;    // work-item counter, zeroed before the launch
+    int *err;       // set when a wait gave up
+    int epoch;
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// one thread: poll until node's flag holds this launch's epoch (bounded)
+__device__ __forceinline__ void dep_wait(const DepArgs &dp, int node)
+{
+    const int *f = dp.flag + node;
+    for (int it = 0; it < DEP_WAIT_LIMIT; it++) {
+        if (ld_acquire_gpu(f) == dp.epoch) return;
+        __nanosleep(100);
+    }
+    atomicExch(dp.err, 1);
+}
+// one thread, after a block barrier that follows every write of the item
+__device__ __forceinline__ void dep_publish(const DepArgs &dp, int node)
+{
+    __threadfence();
+    st_release_gpu(dp.flag + node, dp.epoch);
+}
+
+// Interpolative decompositions of the 2D nodes at level >= 2, one CTA of 128 threads per node,
+// thread `tid` owning candidate row tid (its row of A = K(candidate - c, proxies) in
+// registers). LEAVES: every leaf (candidates = its points; at most 128). Otherwise every
+// internal node in one dependency-ordered launch (candidates = the children's skeletons):
+// items in decreasing node id (deepest level first), so a node's internal children come
+// before it; it waits for their flags and reads their ranks, skeletons and coefficients
+// through L2. When the children's ranks add up to more than 128, thread tid also owns row
+// 128 + tid, kept in global memory (in the node's first U rows, unused until the end).
+// Column-pivoted Gram-Schmidt until the largest residual row norm is <= tol * the largest
+// initial one (ties: the lower row); the dot products of every step are kept in shared
+// memory (row-major, stride MAXR + 1), R11 is gathered from the pivot rows into shared
+// memory, and the back substitution U = [I ; R11^-1 R12]^T runs there. Then U goes out to
+// global memory, with the skeleton and the rank, and the upward coefficients
+// y0 = U^T (the leaf's [1 | x] | the children's y0) are summed by all threads in a fixed order.
+constexpr int ID2_THREADS = 128;
+constexpr int ID2_MAX_ROWS = 2 * ID2_THREADS;   // four children of rank MAXR
+constexpr int ID2_DSTRIDE = Dim<2>::MAXR + 1;
+constexpr size_t ID2_SMEM = sizeof(float) * ID2_THREADS * ID2_DSTRIDE;   // dot products
+
+template <bool LEAVES>
+__global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
+{
+    constexpr int P = Dim<2>::NPROXY, MAXR = Dim<2>::MAXR, NW = ID2_THREADS / 32;
+    static_assert(ID2_MAX_ROWS >= 4 * MAXR && P == MAXR, "overflow rows reuse U rows of MAXR floats");
+    extern __shared__ float dots[];            // [ID2_THREADS][ID2_DSTRIDE]
     __shared__ float prox[P * 2];
     __shared__ float qsh[P];
-    __shared__ float R11[MAXR * MAXR];
+    __shared__ float rdiag[MAXR];
+    __shared__ int piv[MAXR];
+    __shared__ float R11[MAXR * (MAXR + 1) / 2];   // column jj at jj (jj + 1) / 2
+    __shared__ float4 sin_[LEAVES ? ID2_THREADS : ID2_MAX_ROWS];
+    __shared__ float4 part[ID2_THREADS];
     __shared__ float s_bv[2][NW];
     __shared__ int s_bi[2][NW];
-    __shared__ float s_rr;
-    __shared__ int s_crank[8], s_cfirst;
-
+    __shared__ float s_lmax[NW];
+    __shared__ int s_crank[4], s_item;
+    const TreeView &tv = g.tv;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (!LEAVES && tid == 0) s_item = atomicAdd(dp.ticket, 1);
+    __syncthreads();
+    const int item = LEAVES ? (int)blockIdx.x : s_item;
+    if (item >= n_item) return;
+    const int t = items[LEAVES ? item : n_item - 1 - item];
+    const int lvl = tv.level[t];
+    const float2 *xt = (const float2 *)g.xt;
+    float2 *skel = (float2 *)g.skel;
+    const int cfirst = tv.fchild[t], nch = LEAVES ? 0 : tv.nchild[t];
+    if (!LEAVES && tid < nch) {
+        if (!tv.leaf[cfirst + tid]) dep_wait(dp, cfirst + tid);   // leaves: the launch before
+        s_crank[tid] = __ldcg(g.rank + cfirst + tid);
+    }
+    __syncthreads();
     int m = 0;
     if (LEAVES) m = tv.end[t] - tv.start[t];
-    else {
-        if (tid == 0) s_cfirst = tv.fchild[t];
-        for (int c = 0; c < tv.nchild[t]; c++) {
-            const int rc = g.rank[tv.fchild[t] + c];
-            if (tid == 0) s_crank[c] = rc;
-            m += rc;
-        }
-    }
+    else for (int c = 0; c < nch; c++) m += s_crank[c];
+    const int s0 = tv.start[t];
     const long long roff = g.rowoff[t];
     float *U = g.U + roff * MAXR;
     const double h = tv.info->radius / (double)(1LL << lvl);
-    for (int p = tid; p < P; p += ID_THREADS) proxy_point<2>(p, h, prox + p * 2);
+    for (int p = tid; p < P; p += ID2_THREADS) proxy_point<2>(p, h, prox + p * 2);
     const float cx = (float)(tv.info->corner[0] + (double)(2 * tv.ix[(size_t)t * 3 + 0] + 1) * h);
     const float cy = (float)(tv.info->corner[1] + (double)(2 * tv.ix[(size_t)t * 3 + 1] + 1) * h);
+    // candidates and the upward-pass inputs
+    float2 x = make_float2(0.f, 0.f), xx = make_float2(0.f, 0.f);
+    for (int q = 0; q < 2; q++) {
+        const int a = tid + ID2_THREADS * q;
+        if (a >= m) break;
+        float2 pt;
+        if (LEAVES) {
+            pt = xt[s0 + a];
+            sin_[a] = make_float4(1.f, pt.x, pt.y, 0.f);
+        } else {
+            int c = 0, aa = a;
+            while (aa >= s_crank[c]) { aa -= s_crank[c]; c++; }
+            pt = __ldcg(skel + (size_t)(cfirst + c) * MAXR + aa);
+            sin_[a] = __ldcg(g.y0 + (size_t)(cfirst + c) * MAXR + aa);
+        }
+        if (q == 0) x = pt; else xx = pt;
+    }
     __syncthreads();
 
-    float row[RPT][P];
-    float nrm[RPT];
-    V2 x[RPT];
-    int pos[RPT];
-    float lmax = 0.f;
-#pragma unroll
-    for (int j = 0; j < RPT; j++) {
-        const int a = tid + ID_THREADS * j;
-        pos[j] = a < m ? -1 : -2;
-        x[j] = make_float2(0.f, 0.f);
-        if (a < m) {
-            if (LEAVES) x[j] = xt[tv.start[t] + a];
-            else {
-                int c = 0, aa = a;
-                while (aa >= s_crank[c]) { aa -= s_crank[c]; c++; }
-                x[j] = skel[(size_t)(s_cfirst + c) * MAXR + aa];
-            }
-        }
-        const float rx = x[j].x - cx, ry = x[j].y - cy;
-        float s2 = 0.f;
+    const bool valid = tid < m;
+    const bool big = !LEAVES && m > ID2_THREADS;   // uniform over the block
+    const bool xvalid = big && ID2_THREADS + tid < m;
+    float row[P];
+    int pos = valid ? -1 : -2, xpos = xvalid ? -1 : -2;
+    float nrm = -1.f, xnrm = -1.f, lmax = 0.f;
+    {
+        const float rx = x.x - cx, ry = x.y - cy;
+        float s4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int p = 0; p < P; p++) {
             const float dx = rx - prox[2 * p], dy = ry - prox[2 * p + 1];
-            const float w = a < m ? rkernel(fmaf(dx, dx, dy * dy)) : 0.f;
-            row[j][p] = w;
-            s2 = fmaf(w, w, s2);
+            const float w = valid ? rkernel(fmaf(dx, dx, dy * dy)) : 0.f;
+            row[p] = w;
+            s4[p & 3] = fmaf(w, w, s4[p & 3]);
         }
-        nrm[j] = a < m ? s2 : -1.f;
-        lmax = fmaxf(lmax, s2);
+        if (valid) nrm = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+        lmax = fmaxf(lmax, fmaxf(nrm, 0.f));
     }
-    // largest initial norm, and the first pivot proposal
-    float bv = -1.f;
-    int bi = INT_MAX;
-#pragma unroll
-    for (int j = 0; j < RPT; j++)
-        if (nrm[j] > bv) { bv = nrm[j]; bi = tid + ID_THREADS * j; }
+    float *xr = U + (size_t)tid * MAXR;   // overflow row, in the node's first U rows
+    if (xvalid) {
+        const float qx = xx.x - cx, qy = xx.y - cy;
+        float z2 = 0.f;
+        for (int p = 0; p < P; p++) {
+            const float dx = qx - prox[2 * p], dy = qy - prox[2 * p + 1];
+            const float w = rkernel(fmaf(dx, dx, dy * dy));
+            xr[p] = w;
+            z2 = fmaf(w, w, z2);
+        }
+        xnrm = z2;
+        lmax = fmaxf(lmax, z2);
+    }
+    float bv = nrm;
+    int bi = valid ? tid : INT_MAX;
+    if (xnrm > bv) { bv = xnrm; bi = ID2_THREADS + tid; }
     for (int o = 16; o > 0; o >>= 1) {
         lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
         const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
         const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
         if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
-    __shared__ float s_lmax[NW];
     if (lane == 0) { s_lmax[wid] = lmax; s_bv[0][wid] = bv; s_bi[0][wid] = bi; }
     __syncthreads();
     float n0 = 0.f;
     for (int w = 0; w < NW; w++) n0 = fmaxf(n0, s_lmax[w]);
     const float stop2 = g.tol2 * n0;
     const int rmax = min(min(m, P), MAXR);
+    float *drow = dots + (size_t)tid * ID2_DSTRIDE;
     int r = 0, buf = 0;
     while (r < rmax) {
-        // every thread reads the same partials: the same pivot everywhere
         float v = s_bv[buf][0];
         int best = s_bi[buf][0];
         for (int w = 1; w < NW; w++)
             if (s_bv[buf][w] > v || (s_bv[buf][w] == v && s_bi[buf][w] < best)) { v = s_bv[buf][w]; best = s_bi[buf][w]; }
         if (best == INT_MAX || !(v > stop2) || !(v > 0.f)) break;
-        const int owner = best % ID_THREADS, jb = best / ID_THREADS;
-        if (tid == owner) {
+        if (best == tid) {
+            const float rr = sqrtf(nrm);
+            const float inv = 1.0f / rr;
 #pragma unroll
-            for (int j = 0; j < RPT; j++)
-                if (j == jb) {
-                    const float rr = sqrtf(nrm[j]);
-                    const float inv = 1.0f / rr;
-#pragma unroll
-                    for (int p = 0; p < P; p++) qsh[p] = row[j][p] * inv;
-                    s_rr = rr;
-                    pos[j] = r;
-                    nrm[j] = -1.f;
-                }
+            for (int p = 0; p < P; p++) qsh[p] = row[p] * inv;
+            rdiag[r] = rr;
+            piv[r] = best;
+            pos = r;
+            nrm = -1.f;
+        } else if (best == ID2_THREADS + tid) {
+            const float rr = sqrtf(xnrm);
+            const float inv = 1.0f / rr;
+            for (int p = 0; p < P; p++) qsh[p] = xr[p] * inv;
+            rdiag[r] = rr;
+            piv[r] = best;
+            xpos = r;
+            xnrm = -1.f;
         }
-        for (int k = tid; k < r; k += ID_THREADS) R11[k * MAXR + r] = U[(size_t)best * MAXR + k];
         __syncthreads();
-        if (tid == 0) R11[r * MAXR + r] = s_rr;
         bv = -1.f;
         bi = INT_MAX;
+        if (pos == -1) {
+            float d4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int j = 0; j < RPT; j++) {
-            if (pos[j] != -1) continue;
+            for (int p = 0; p < P; p++) d4[p & 3] = fmaf(qsh[p], row[p], d4[p & 3]);
+            const float dot = (d4[0] + d4[1]) + (d4[2] + d4[3]);
+            float s4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                row[p] = fmaf(-dot, qsh[p], row[p]);
+                s4[p & 3] = fmaf(row[p], row[p], s4[p & 3]);
+            }
+            nrm = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            drow[r] = dot;
+            bv = nrm;
+            bi = tid;
+        }
+        if (xpos == -1) {
             float dot = 0.f;
-#pragma unroll
-            for (int p = 0; p < P; p++) dot = fmaf(qsh[p], row[j][p], dot);
+            for (int p = 0; p < P; p++) dot = fmaf(qsh[p], xr[p], dot);
             float s2 = 0.f;
-#pragma unroll
-            for (int p = 0; p < P; p++) { row[j][p] = fmaf(-dot, qsh[p], row[j][p]); s2 = fmaf(row[j][p], row[j][p], s2); }
-            nrm[j] = s2;
-            U[(size_t)(tid + ID_THREADS * j) * MAXR + r] = dot;
-            if (s2 > bv) { bv = s2; bi = tid + ID_THREADS * j; }
+            for (int p = 0; p < P; p++) {
+                const float y = fmaf(-dot, qsh[p], xr[p]);
+                xr[p] = y;
+                s2 = fmaf(y, y, s2);
+            }
+            xnrm = s2;
+            U[(size_t)(ID2_THREADS + tid) * MAXR + r] = dot;
+            if (s2 > bv) { bv = s2; bi = ID2_THREADS + tid; }
         }
         for (int o = 16; o > 0; o >>= 1) {
             const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -940,48 +1058,68 @@ __global__ void __launch_bounds__(ID_THREADS, RPT == 1 ? 4 : 2) k_id_reg(int lev
         __syncthreads();
     }
     __syncthreads();
-#pragma unroll
-    for (int j = 0; j < RPT; j++)
-        if (pos[j] >= 0) skel[(size_t)t * MAXR + pos[j]] = x[j];
+    // skeleton and rank; R11 from the pivot rows' dot products (column jj: its entries k < jj)
+    if (pos >= 0) skel[(size_t)t * MAXR + pos] = x;
+    if (xpos >= 0) skel[(size_t)t * MAXR + xpos] = xx;
     if (tid == 0) g.rank[t] = r;
-#pragma unroll
-    for (int j = 0; j < RPT; j++) {
-        const int a = tid + ID_THREADS * j;
-        if (a >= m) continue;
-        float *u = U + (size_t)a * MAXR;
-        if (pos[j] >= 0) {
-            for (int k = 0; k < r; k++) u[k] = (k == pos[j]) ? 1.f : 0.f;
-        } else {
-            for (int k = r - 1; k >= 0; k--) {
-                float acc = u[k];
-                for (int jj = k + 1; jj < r; jj++) acc = fmaf(-R11[k * MAXR + jj], u[jj], acc);
-                u[k] = acc / R11[k * MAXR + k];
-            }
+    for (int idx = tid; idx < r * r; idx += ID2_THREADS) {
+        const int jj = idx / r, k = idx % r;
+        if (k > jj) continue;
+        const int pr = piv[jj];
+        R11[jj * (jj + 1) / 2 + k] = k == jj ? rdiag[jj]
+                                             : (pr < ID2_THREADS ? dots[(size_t)pr * ID2_DSTRIDE + k]
+                                                                 : U[(size_t)pr * MAXR + k]);
+    }
+    __syncthreads();
+    // back substitution of the non-pivot rows
+    if (pos == -1) {
+        for (int k = r - 1; k >= 0; k--) {
+            float acc = drow[k];
+            for (int jj = k + 1; jj < r; jj++) acc = fmaf(-R11[jj * (jj + 1) / 2 + k], drow[jj], acc);
+            drow[k] = acc / R11[k * (k + 1) / 2 + k];
+        }
+    }
+    if (xpos == -1) {
+        float *u = U + (size_t)(ID2_THREADS + tid) * MAXR;
+        for (int k = r - 1; k >= 0; k--) {
+            float acc = u[k];
+            for (int jj = k + 1; jj < r; jj++) acc = fmaf(-R11[jj * (jj + 1) / 2 + k], u[jj], acc);
+            u[k] = acc / R11[k * (k + 1) / 2 + k];
         }
     }
     __syncthreads();
-    // upward pass of this node: y0[t] = U^T (the leaf's [1 | x] | the children's y0)
-    for (int k = tid; k < r; k += ID_THREADS) {
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (LEAVES) {
-            for (int a = 0; a < m; a++) {
-                const float w = U[(size_t)a * MAXR + k];
-                const V2 xa = xt[tv.start[t] + a];
-                acc.x += w;
-                acc.y = fmaf(w, xa.x, acc.y);
-                acc.z = fmaf(w, xa.y, acc.z);
-            }
-        } else {
-            int a = 0;
-            for (int c = 0; c < tv.nchild[t]; c++)
-                for (int kk = 0; kk < s_crank[c]; kk++, a++) {
-                    const float w = U[(size_t)a * MAXR + k];
-                    const float4 y = g.y0[(size_t)(s_cfirst + c) * MAXR + kk];
-                    acc.x = fmaf(w, y.x, acc.x); acc.y = fmaf(w, y.y, acc.y);
-                    acc.z = fmaf(w, y.z, acc.z); acc.w = fmaf(w, y.w, acc.w);
-                }
+    // pivot rows are rows of the identity
+    if (pos >= 0)
+        for (int k = 0; k < r; k++) drow[k] = k == pos ? 1.f : 0.f;
+    if (xpos >= 0)
+        for (int k = 0; k < r; k++) U[(size_t)(ID2_THREADS + tid) * MAXR + k] = k == xpos ? 1.f : 0.f;
+    __syncthreads();
+    // U rows 0 .. min(m, 128) - 1 out of shared memory (over the overflow rows' scratch)
+    const int mm = min(m, ID2_THREADS);
+    for (int idx = tid; idx < mm * r; idx += ID2_THREADS) {
+        const int a = idx / r, k = idx % r;
+        U[(size_t)a * MAXR + k] = dots[(size_t)a * ID2_DSTRIDE + k];
+    }
+    // y0[k] = sum_a U[a][k] in[a]: groups of RG threads over k, C = 128 / RG groups over a
+    const int RG = r <= 16 ? 16 : (r <= 32 ? 32 : 64);
+    const int C = ID2_THREADS / RG, kk = tid % RG, cg = tid / RG;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (kk < r) {
+        for (int a = cg; a < m; a += C) {
+            const float w = a < ID2_THREADS ? dots[(size_t)a * ID2_DSTRIDE + kk] : U[(size_t)a * MAXR + kk];
+            fma4(acc, w, sin_[a]);
         }
-        g.y0[(size_t)t * MAXR + k] = acc;
+    }
+    part[tid] = acc;
+    __syncthreads();
+    if (tid < r) {
+        float4 y = part[tid];
+        for (int c = 1; c < C; c++) add4(y, part[c * RG + tid]);
+        g.y0[(size_t)t * MAXR + tid] = y;
+    }
+    if (!LEAVES) {
+        __syncthreads();
+        if (tid == 0) dep_publish(dp, t);
     }
 }
 
@@ -1014,12 +1152,6 @@ __device__ __forceinline__ float4 input_at(const ProdArgs &g, const typename Dim
 {
     return g.xin ? g.xin[j] : with_one<D>(xt[j]);
 }
-__device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
-{
-    acc.x = fmaf(w, v.x, acc.x); acc.y = fmaf(w, v.y, acc.y);
-    acc.z = fmaf(w, v.z, acc.z); acc.w = fmaf(w, v.w, acc.w);
-}
-__device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
 
 // upward pass, one warp per node of `level`: y0[t] = U_t^T (leaf points | children's y0)
 template <int D>
@@ -1366,7 +1498,9 @@ public:
         blkcnt_.exact((size_t)ceil_div(n, TREE_BLOCK) * 64);
         blkoff_.exact((size_t)ceil_div(n, TREE_BLOCK) * 64);
         btot_.exact(32);
+        ticket_.exact(1);
         info_.exact(1);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(info_.p, 0, sizeof(TreeInfo), st_));
         size_t b1 = 0, b2 = 0;
         TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, b1, keys_in_.p, keys_.p, idx_in_.p,
                                                         perm_.p, n, 0, D * Dim<D>::L, st_));
@@ -1381,6 +1515,8 @@ public:
                                              (int)id_smem_bytes<D>(id_mcap())));
         TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)id_smem_bytes<D>(id_mcap())));
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ID2_SMEM));
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ID2_SMEM));
     }
 
     int build(const void *Y, int leaf_size, double tol) override
@@ -1420,9 +1556,15 @@ public:
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + cap_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&hint_, ipos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&hleaf_, lpos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
             const TreeInfo &I = *hinfo_.p;
             if (I.nonfinite) return -1;
+            if (I.pad[1]) {   // a dependency wait of the previous build gave up
+                fprintf(stderr, "tsne_h2pack: H2 basis construction lost a dependency wait\n");
+                return -1;
+            }
             if (I.pad[0]) {   // node table full: grow and start over
                 cap_node_ *= 2;
                 alloc_nodes();
@@ -1486,10 +1628,27 @@ public:
         IdArgs il{view(), xt_.p, skel_.p, rank_.p, rowoff_.p, U_.p, gA_.p, gnrm_.p, gsel_.p, gcand_.p, mleaf, tol2,
                   y0_.p};
         const int first = I.level_begin[MIN_ADM_LEVEL];
-        if (D == 2 && stats_.max_leaf <= ID_THREADS)
-            k_id_reg<true, 1><<<n_node_ - first, ID_THREADS, 0, st_>>>(MIN_ADM_LEVEL, il);
-        else
-            k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
+        if (D == 2 && stats_.max_leaf <= ID2_THREADS) {
+            // leaves in one launch, then the internal nodes of every level in one
+            // dependency-ordered launch
+            DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
+            if (hleaf_ > 0) k_id2d<true><<<hleaf_, ID2_THREADS, ID2_SMEM, st_>>>(hleaf_, llist_.p, il, dp);
+            mark_end(t_bases, 2);
+            t_bases = mark_begin();
+            if (hint_ > 0) {
+                TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
+                k_id2d<false><<<hint_, ID2_THREADS, ID2_SMEM, st_>>>(hint_, ilist_.p, il, dp);
+            }
+            launches_ += 2;
+            mark_end(t_bases, 7);
+            if (timing_) TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+            sec_end("lists+bases");
+            built_ = true;
+            y0_from_build_ = true;
+            rank_stats_valid_ = false;
+            return 0;
+        }
+        k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
         launches_++;
         mark_end(t_bases, 2);
         t_bases = mark_begin();
@@ -1499,8 +1658,7 @@ public:
         for (int l = max_level_ - 1; l >= MIN_ADM_LEVEL; l--) {
             const int nl = I.n_level_nodes[l];
             if (nl == 0) continue;
-            if (D == 2) k_id_reg<false, 2><<<nl, ID_THREADS, 0, st_>>>(l, ia);
-            else k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia);
+            k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia);
             launches_++;
         }
         mark_end(t_bases, 7);
@@ -1526,11 +1684,17 @@ public:
             launches_++;
         }
         k_lists_leaves<D><<<148 * 8, 128, 0, st_>>>(view(), lo);
-        k_rowcap<D><<<148 * 4, 256, 0, st_>>>(view(), rowcap_.p);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(iflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
+        TSNE_CUDA_CHECK(cudaMemsetAsync(lflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
+        k_rowcap<D><<<148 * 4, 256, 0, st_>>>(view(), rowcap_.p, iflag_.p, lflag_.p);
         scan_exclusive(far_cnt_.p, far_ptr_.p, cap_node_);
         scan_exclusive(near_cnt_.p, near_ptr_.p, cap_node_);
         scan_exclusive_ll(rowcap_.p, rowoff_.p, cap_node_);
-        launches_ += 5;
+        scan_exclusive(iflag_.p, ipos_.p, cap_node_);
+        scan_exclusive(lflag_.p, lpos_.p, cap_node_);
+        k_flag_list<<<148 * 4, 256, 0, st_>>>(&info_.p->n_node, iflag_.p, ipos_.p, ilist_.p);
+        k_flag_list<<<148 * 4, 256, 0, st_>>>(&info_.p->n_node, lflag_.p, lpos_.p, llist_.p);
+        launches_ += 10;
     }
 
     void alloc_lists()
@@ -1541,6 +1705,8 @@ public:
         far_cnt_.exact(c + 1); near_cnt_.exact(c + 1);
         far_ptr_.exact(c + 2); near_ptr_.exact(c + 2);
         rowcap_.exact(c + 1);
+        iflag_.exact(c + 1); ipos_.exact(c + 2); ilist_.exact(c + 1);
+        lflag_.exact(c + 1); lpos_.exact(c + 2); llist_.exact(c + 1);
         rowoff_.exact(c + 2);
     }
 
@@ -1713,6 +1879,8 @@ private:
         start_.exact(c); end_.exact(c); level_.exact(c); parent_.exact(c); fchild_.exact(c);
         nchild_.exact(c); leaf_.exact(c); ix_.exact(3 * c);
         bset_.exact(c * (Dim<D>::L + 1));
+        flag_.exact(c);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(flag_.p, 0, sizeof(int) * c, st_));
         nid_.exact(c * (Dim<D>::L + 1));
         alloc_lists();
     }
@@ -1817,8 +1985,13 @@ private:
     DevBuf<int> start_, end_, level_, parent_, fchild_, nchild_, leaf_, ix_;
     DevBuf<signed char> delta_;
     DevBuf<int> fm_, blkcnt_, blkoff_, bset_, nid_, btot_;
+    DevBuf<int> flag_, ticket_;   // dependency-ordered launches
+    int epoch_ = 0;
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;
     DevBuf<int> rowcap_;
+    DevBuf<int> iflag_, ipos_, ilist_;   // internal nodes at level >= 2, in increasing id
+    DevBuf<int> lflag_, lpos_, llist_;   // leaves at level >= 2, in increasing id
+    int hint_ = 0, hleaf_ = 0;
     DevBuf<long long> rowoff_;
     DevBuf<int> rank_;
     DevBuf<Vec<D>> skel_;

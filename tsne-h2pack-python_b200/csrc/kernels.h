@@ -66,14 +66,9 @@ void launch_permute_int(cudaStream_t st, int n, const int *ord, const int *src, 
                         int identity_src);
 void launch_invert_perm(cudaStream_t st, int n, const int *ord, int *inv);
 void launch_row_len(cudaStream_t st, int n, const int *ord, const int *rp_old, int *len_new);
-// renumbering of the CSR (new row k = old row ord[k]) as two stable transposes: row copy
-// with keys = new column, (row, value) swap after the first sort, unpack after the second
-void launch_row_copy(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
-                     const int *col_old, const float *val_old, const int *rp_new, unsigned int *key,
-                     unsigned long long *pack);
-void launch_swap_pack(cudaStream_t st, long long nnz, const unsigned int *key_in, const unsigned long long *pack_in,
-                      unsigned int *key_out, unsigned long long *pack_out);
-void launch_unpack(cudaStream_t st, long long nnz, const unsigned long long *pack, int *col, float *val);
+// renumbering of the CSR: new row k = old row ord[k], columns mapped through inv
+void launch_row_gather(cudaStream_t st, int n, const int *ord, const int *inv, const int *rp_old,
+                       const int *col_old, const float *val_old, const int *rp_new, int *col_new, float *val_new);
 void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist,
                  double perplexity, double *out);
 

@@ -54,11 +54,6 @@ struct TreeView {
     TreeInfo *info;
 };
 
-__device__ __forceinline__ int digit_of(unsigned long long key, int shift, int nchm1)
-{
-    return (int)((key >> shift) & (unsigned long long)nchm1);
-}
-
 // ---------------------------------------------------------------------------------
 // root box and keys
 // ---------------------------------------------------------------------------------
@@ -327,7 +322,12 @@ __global__ void __launch_bounds__(1024) k_tree_scan(int nblk, TreeView tv)
         info->level_begin[32] = acc;
         info->n_node = acc;
         info->max_level = maxl;
-        if (acc > tv.cap_node) info->pad[0] = 1;
+        if (acc > tv.cap_node) {   // node table full: the host regrows it; nothing downstream runs
+            info->pad[0] = 1;
+            info->n_node = 0;
+            info->max_level = 0;
+            for (int l = 0; l < 32; l++) info->n_level_nodes[l] = 0;
+        }
     }
 }
 
@@ -414,6 +414,51 @@ __global__ void k_tree_finish(TreeView tv)
             tv.nchild[t] = c;
         }
     }
+}
+
+// ---------------------------------------------------------------------------------
+// dependency-ordered launches
+//
+// A kernel that processes the nodes of several levels in one launch takes its work items from
+// a ticket counter, so items start in ticket order whatever order the hardware dispatches
+// blocks in. An item waits only for items with smaller tickets, which are held by running
+// blocks or finished, so every wait ends. The waits are bounded all the same: after
+// DEP_WAIT_LIMIT polls the waiting thread records the failure (the host reports it) and goes on.
+// ---------------------------------------------------------------------------------
+constexpr int DEP_WAIT_LIMIT = 1 << 22;
+
+struct DepArgs {
+    int *flag;      // per node: epoch of the last launch that finished it
+    int *ticket;    // work-item counter, zeroed before the launch
+    int *err;       // set when a wait gave up
+    int epoch;
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// one thread: poll until node's flag holds this launch's epoch (bounded)
+__device__ __forceinline__ void dep_wait(const DepArgs &dp, int node)
+{
+    const int *f = dp.flag + node;
+    for (int it = 0; it < DEP_WAIT_LIMIT; it++) {
+        if (ld_acquire_gpu(f) == dp.epoch) return;
+        __nanosleep(100);
+    }
+    atomicExch(dp.err, 1);
+}
+// one thread, after a block barrier that follows every write of the item
+__device__ __forceinline__ void dep_publish(const DepArgs &dp, int node)
+{
+    __threadfence();
+    st_release_gpu(dp.flag + node, dp.epoch);
 }
 
 // ---------------------------------------------------------------------------------
@@ -511,13 +556,78 @@ __device__ void process_target(const TreeView &tv, ListOut &lo, int t)
     }
 }
 
-// count pass, internal targets of one level (their NSET feeds the next level)
+// count pass of the internal targets of every level in one dependency-ordered launch
+// (persistent warps; a warp per target, in increasing node id, so a target's parent comes
+// first). For target t the lanes take the entries a of the parent's inadmissible set, each
+// with its candidate children c (the entry itself when it is a leaf): c goes to the far list
+// when c != t and (t, c) is admissible, else to t's inadmissible set, which is written in
+// (a, c) order, as process_target does.
 template <int D>
-__global__ void __launch_bounds__(128) k_lists_level(int l, TreeView tv, ListOut lo)
+__global__ void __launch_bounds__(256) k_lists_internal(TreeView tv, ListOut lo, DepArgs dp)
 {
-    const int lb = tv.info->level_begin[l], nl = tv.info->n_level_nodes[l];
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x)
-        if (!tv.leaf[lb + j]) process_target<D>(tv, lo, lb + j);
+    constexpr int NCH = 1 << D;
+    const int lane = threadIdx.x & 31;
+    const int n_node = tv.info->n_node;
+    const int cap = tv.nset_cap;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(dp.ticket, 1);
+        const int t = __shfl_sync(0xffffffffu, item, 0);
+        if (t >= n_node) break;
+        if (tv.leaf[t]) continue;
+        int nf = 0, ns = 0;
+        if (t == 0) {
+            if (lane == 0) lo.nset[0] = 0;
+            ns = 1;
+        } else {
+            const int p = tv.parent[t];
+            if (lane == 0) dep_wait(dp, p);
+            __syncwarp();
+            const int pn = __ldcg(lo.nset_cnt + p);
+            for (int a0 = 0; a0 < pn; a0 += 32) {
+                const int a = a0 + lane;
+                int c0 = 0, c1 = 0, nn = 0;
+                if (a < pn) {
+                    const int src = __ldcg(lo.nset + (size_t)p * cap + a);
+                    const bool sl = tv.leaf[src] != 0;
+                    c0 = sl ? src : tv.fchild[src];
+                    c1 = sl ? src + 1 : tv.fchild[src] + tv.nchild[src];
+                }
+#pragma unroll
+                for (int k = 0; k < NCH; k++) {
+                    const int c = c0 + k;
+                    if (c < c1) {
+                        if (c != t && admissible<D>(tv, t, c)) nf++;
+                        else nn++;
+                    }
+                }
+                int inc = nn;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += y;
+                }
+                int w = ns + inc - nn;
+#pragma unroll
+                for (int k = 0; k < NCH; k++) {
+                    const int c = c0 + k;
+                    if (c < c1 && !(c != t && admissible<D>(tv, t, c))) {
+                        if (w < cap) lo.nset[(size_t)t * cap + w] = c;
+                        w++;
+                    }
+                }
+                ns += __shfl_sync(0xffffffffu, inc, 31);
+            }
+        }
+        nf = warp_sum(nf);
+        if (lane == 0) {
+            lo.far_cnt[t] = nf;
+            lo.near_cnt[t] = 0;
+            if (ns > cap) { atomicExch(&tv.info->nset_overflow, 1); ns = cap; }
+            lo.nset_cnt[t] = ns;
+        }
+        __syncwarp();
+        if (lane == 0) dep_publish(dp, t);
+    }
 }
 
 // count pass, every leaf target (leaves need only their parent's NSET)
@@ -816,50 +926,6 @@ __device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
 }
 __device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
 
-// ---------------------------------------------------------------------------------
-// dependency-ordered launches
-//
-// A kernel that processes the nodes of several levels in one launch takes its work items from
-// a ticket counter, so items start in ticket order whatever order the hardware dispatches
-// blocks in. An item waits only for items with smaller tickets, which are held by running
-// blocks or finished, so every wait ends. The waits are bounded all the same: after
-// DEP_WAIT_LIMIT polls the waiting thread records the failure (the host reports it) and goes on.
-// ---------------------------------------------------------------------------------
-constexpr int DEP_WAIT_LIMIT = 1 << 22;
-
-struct DepArgs {
-    int *flag;      // per node: epoch of the last launch that finished it
-    int *ticket;    // work-item counter, zeroed before the launch
-    int *err;       // set when a wait gave up
-    int epoch;
-};
-
-__device__ __forceinline__ int ld_acquire_gpu(const int *p)
-{
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_gpu(int *p, int v)
-{
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-// one thread: poll until node's flag holds this launch's epoch (bounded)
-__device__ __forceinline__ void dep_wait(const DepArgs &dp, int node)
-{
-    const int *f = dp.flag + node;
-    for (int it = 0; it < DEP_WAIT_LIMIT; it++) {
-        if (ld_acquire_gpu(f) == dp.epoch) return;
-        __nanosleep(100);
-    }
-    atomicExch(dp.err, 1);
-}
-// one thread, after a block barrier that follows every write of the item
-__device__ __forceinline__ void dep_publish(const DepArgs &dp, int node)
-{
-    __threadfence();
-    st_release_gpu(dp.flag + node, dp.epoch);
-}
 
 // Interpolative decompositions of the 2D nodes at level >= 2, one CTA of 128 threads per node,
 // thread `tid` owning candidate row tid (its row of A = K(candidate - c, proxies) in
@@ -1410,54 +1476,85 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
     }
 }
 
-// LEAVES = false: the internal nodes of `level` (run top-down); true: every leaf at level >= 2
-// (after all internal levels)
-template <int D, bool LEAVES>
-__global__ void __launch_bounds__(256) k_down(int level, ProdArgs g)
+// downward pass of node t (one warp): the node's y1 through U onto its leaf points (yp) or
+// its children's y1. FRESH: y1 is read through L2 (written in the same launch).
+template <int D, bool FRESH>
+__device__ __forceinline__ void down_node(const ProdArgs &g, int t, int lane)
 {
     constexpr int MAXR = Dim<D>::MAXR;
     const TreeView &tv = g.tv;
-    const int lb = tv.info->level_begin[level];
-    const int nl = LEAVES ? tv.info->n_node - lb : tv.info->n_level_nodes[level];
+    const int r = g.rank[t];
+    const float *U = g.U + g.rowoff[t] * MAXR;
+    float4 yr[MAXR / 32];
+    for (int h = 0; h < MAXR / 32; h++) {
+        const int k = lane + 32 * h;
+        const float4 *src = g.y1 + (size_t)t * MAXR + k;
+        yr[h] = k < r ? (FRESH ? __ldcg(src) : *src) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const bool isleaf = tv.leaf[t] != 0;
+    int m = 0;
+    if (isleaf) m = tv.end[t] - tv.start[t];
+    else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
+    for (int a0 = 0; a0 < m; a0 += 32) {
+        const int a = a0 + lane;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int k = 0; k < r; k++) {
+            const float4 y = make_float4(__shfl_sync(0xffffffffu, yr[k >> 5].x, k & 31),
+                                         __shfl_sync(0xffffffffu, yr[k >> 5].y, k & 31),
+                                         __shfl_sync(0xffffffffu, yr[k >> 5].z, k & 31),
+                                         __shfl_sync(0xffffffffu, yr[k >> 5].w, k & 31));
+            if (a < m) fma4(acc, U[(size_t)a * MAXR + k], y);
+        }
+        if (a < m) {
+            if (isleaf) {
+                float4 o = g.yp[tv.start[t] + a];
+                add4(o, acc);
+                g.yp[tv.start[t] + a] = o;
+            } else {
+                int c = tv.fchild[t], aa = a;
+                while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
+                float4 *dst = g.y1 + (size_t)c * MAXR + aa;
+                float4 o = FRESH ? __ldcg(dst) : *dst;
+                add4(o, acc);
+                *dst = o;
+            }
+        }
+    }
+}
+
+// downward pass of every internal node at level >= 2 in one dependency-ordered launch
+// (persistent warps, items in increasing node id): a node waits for its parent's push
+template <int D>
+__global__ void __launch_bounds__(256) k_down_internal(int n_item, const int *__restrict__ items, ProdArgs g,
+                                                        DepArgs dp)
+{
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(dp.ticket, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= n_item) break;
+        const int t = items[item];
+        const int p = g.tv.parent[t];
+        if (lane == 0 && g.tv.level[p] >= MIN_ADM_LEVEL) dep_wait(dp, p);
+        __syncwarp();
+        down_node<D, true>(g, t, lane);
+        __syncwarp();
+        if (lane == 0) dep_publish(dp, t);
+    }
+}
+
+// downward pass of every leaf at level >= 2 (after the internal nodes)
+template <int D>
+__global__ void __launch_bounds__(256) k_down_leaves(ProdArgs g)
+{
+    const TreeView &tv = g.tv;
+    const int lb = tv.info->level_begin[MIN_ADM_LEVEL];
+    const int nl = tv.info->n_node - lb;
     const int lane = threadIdx.x & 31;
     for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nl; j += (gridDim.x * blockDim.x) >> 5) {
         const int t = lb + j;
-        if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) continue;
-        const int r = g.rank[t];
-        const float *U = g.U + g.rowoff[t] * MAXR;
-        float4 yr[MAXR / 32];
-        for (int h = 0; h < MAXR / 32; h++) {
-            const int k = lane + 32 * h;
-            yr[h] = k < r ? g.y1[(size_t)t * MAXR + k] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        const bool isleaf = tv.leaf[t] != 0;
-        int m = 0;
-        if (isleaf) m = tv.end[t] - tv.start[t];
-        else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
-        for (int a0 = 0; a0 < m; a0 += 32) {
-            const int a = a0 + lane;
-            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int k = 0; k < r; k++) {
-                const float4 y = make_float4(__shfl_sync(0xffffffffu, yr[k >> 5].x, k & 31),
-                                             __shfl_sync(0xffffffffu, yr[k >> 5].y, k & 31),
-                                             __shfl_sync(0xffffffffu, yr[k >> 5].z, k & 31),
-                                             __shfl_sync(0xffffffffu, yr[k >> 5].w, k & 31));
-                if (a < m) fma4(acc, U[(size_t)a * MAXR + k], y);
-            }
-            if (a < m) {
-                if (isleaf) {
-                    float4 o = g.yp[tv.start[t] + a];
-                    add4(o, acc);
-                    g.yp[tv.start[t] + a] = o;
-                } else {
-                    int c = tv.fchild[t], aa = a;
-                    while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
-                    float4 o = g.y1[(size_t)c * MAXR + aa];
-                    add4(o, acc);
-                    g.y1[(size_t)c * MAXR + aa] = o;
-                }
-            }
-        }
+        if (tv.leaf[t]) down_node<D, false>(g, t, lane);
     }
 }
 
@@ -1529,10 +1626,8 @@ public:
         // loop) and the counting pass of the interaction lists (kernels read the level and node
         // counts on the device; scans run over the node capacity, whose unused tail counts are
         // zero), then a single synchronisation reads the tree, the list totals and the basis
-        // rows. A full node table, a tree deeper than the list levels counted or a full
-        // inadmissible-source set are caught there and redone.
+        // rows. A full node table or a full inadmissible-source set are caught there and redone.
         bool tree_ok = false;
-        int list_levels = std::min(L + 1, std::max(6, last_max_level_ + 2));
         for (int attempt = 0; attempt < 12; attempt++) {
             if (!tree_ok) {
                 const int nblk = ceil_div(n_, TREE_BLOCK);
@@ -1551,7 +1646,7 @@ public:
                 launches_ += 9 + 4;
                 tree_ok = true;
             }
-            launch_list_counts(list_levels);
+            launch_list_counts();
             TSNE_CUDA_CHECK(cudaMemcpyAsync(hinfo_.p, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[0], far_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&htot_[1], near_ptr_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
@@ -1569,10 +1664,6 @@ public:
                 cap_node_ *= 2;
                 alloc_nodes();
                 tree_ok = false;
-                continue;
-            }
-            if (list_levels < I.max_level) {   // internal targets below the counted levels
-                list_levels = std::min(L + 1, I.max_level + 1);
                 continue;
             }
             if (I.nset_overflow) {   // inadmissible-source set full: grow, recount
@@ -1670,20 +1761,20 @@ public:
         return 0;
     }
 
-    // counting pass of the lists for levels [0, levels) plus every leaf target, the pointer
+    // counting pass of the lists (internal targets, then every leaf target), the pointer
     // scans and the basis row offsets, all over the node capacity
-    void launch_list_counts(int levels)
+    void launch_list_counts()
     {
         TSNE_CUDA_CHECK(cudaMemsetAsync(far_cnt_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(near_cnt_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(rowcap_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(&info_.p->nset_overflow, 0, sizeof(int), st_));
         ListOut lo = list_out(0);
-        for (int l = 0; l < levels; l++) {
-            k_lists_level<D><<<148 * 2, 128, 0, st_>>>(l, view(), lo);
-            launches_++;
-        }
+        TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
+        DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
+        k_lists_internal<D><<<148 * 4, 256, 0, st_>>>(view(), lo, dp);
         k_lists_leaves<D><<<148 * 8, 128, 0, st_>>>(view(), lo);
+        launches_ += 2;
         TSNE_CUDA_CHECK(cudaMemsetAsync(iflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(lflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         k_rowcap<D><<<148 * 4, 256, 0, st_>>>(view(), rowcap_.p, iflag_.p, lflag_.p);
@@ -1952,11 +2043,13 @@ private:
         mark_end(t_near, 4);
         launches_ += 2;
         cudaEvent_t t_down = mark_begin();
-        for (int l = MIN_ADM_LEVEL; l < max_level_; l++) {
-            const int nl = I.n_level_nodes[l];
-            if (nl > 0) { k_down<D, false><<<grid_for((long long)nl * 32, 256), 256, 0, st_>>>(l, g); launches_++; }
+        if (hint_ > 0) {
+            TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
+            DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
+            k_down_internal<D><<<grid_for((long long)hint_ * 32, 256, 148 * 8), 256, 0, st_>>>(hint_, ilist_.p, g, dp);
+            launches_++;
         }
-        k_down<D, true><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(MIN_ADM_LEVEL, g);
+        k_down_leaves<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(g);
         launches_++;
         mark_end(t_down, 5);
     }

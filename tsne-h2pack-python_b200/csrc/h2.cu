@@ -927,6 +927,16 @@ __device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
 __device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
 
 
+// Warp argmax of (norm, row): the largest norm, ties to the lowest row. Norms are >= 0 or -1
+// (no candidate), so their bit patterns order like the values.
+__device__ __forceinline__ void warp_argmax(float &bv, int &bi)
+{
+    const int key = __float_as_int(bv);
+    const int mx = __reduce_max_sync(0xffffffffu, key);
+    bi = __reduce_min_sync(0xffffffffu, key == mx ? bi : INT_MAX);
+    bv = __int_as_float(mx);
+}
+
 // Interpolative decompositions of the 2D nodes at level >= 2, one CTA of 128 threads per node,
 // thread `tid` owning candidate row tid (its row of A = K(candidate - c, proxies) in
 // registers). LEAVES: every leaf (candidates = its points; at most 128). Otherwise every
@@ -959,6 +969,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     __shared__ float R11[MAXR * (MAXR + 1) / 2];   // column jj at jj (jj + 1) / 2
     __shared__ float4 sin_[LEAVES ? ID2_THREADS : ID2_MAX_ROWS];
     __shared__ float4 part[ID2_THREADS];
+    __shared__ float2 sxy[ID2_MAX_ROWS];
     __shared__ float s_bv[2][NW];
     __shared__ int s_bi[2][NW];
     __shared__ float s_lmax[NW];
@@ -990,7 +1001,6 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     const float cx = (float)(tv.info->corner[0] + (double)(2 * tv.ix[(size_t)t * 3 + 0] + 1) * h);
     const float cy = (float)(tv.info->corner[1] + (double)(2 * tv.ix[(size_t)t * 3 + 1] + 1) * h);
     // candidates and the upward-pass inputs
-    float2 x = make_float2(0.f, 0.f), xx = make_float2(0.f, 0.f);
     for (int q = 0; q < 2; q++) {
         const int a = tid + ID2_THREADS * q;
         if (a >= m) break;
@@ -1004,7 +1014,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
             pt = __ldcg(skel + (size_t)(cfirst + c) * MAXR + aa);
             sin_[a] = __ldcg(g.y0 + (size_t)(cfirst + c) * MAXR + aa);
         }
-        if (q == 0) x = pt; else xx = pt;
+        sxy[a] = pt;
     }
     __syncthreads();
 
@@ -1015,6 +1025,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     int pos = valid ? -1 : -2, xpos = xvalid ? -1 : -2;
     float nrm = -1.f, xnrm = -1.f, lmax = 0.f;
     {
+        const float2 x = valid ? sxy[tid] : make_float2(0.f, 0.f);
         const float rx = x.x - cx, ry = x.y - cy;
         float s4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
@@ -1029,6 +1040,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     }
     float *xr = U + (size_t)tid * MAXR;   // overflow row, in the node's first U rows
     if (xvalid) {
+        const float2 xx = sxy[ID2_THREADS + tid];
         const float qx = xx.x - cx, qy = xx.y - cy;
         float z2 = 0.f;
         for (int p = 0; p < P; p++) {
@@ -1043,12 +1055,8 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     float bv = nrm;
     int bi = valid ? tid : INT_MAX;
     if (xnrm > bv) { bv = xnrm; bi = ID2_THREADS + tid; }
-    for (int o = 16; o > 0; o >>= 1) {
-        lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-    }
+    lmax = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(lmax)));
+    warp_argmax(bv, bi);
     if (lane == 0) { s_lmax[wid] = lmax; s_bv[0][wid] = bv; s_bi[0][wid] = bi; }
     __syncthreads();
     float n0 = 0.f;
@@ -1089,6 +1097,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
 #pragma unroll
             for (int p = 0; p < P; p++) d4[p & 3] = fmaf(qsh[p], row[p], d4[p & 3]);
             const float dot = (d4[0] + d4[1]) + (d4[2] + d4[3]);
+            asm volatile("" ::: "memory");   // reload q below instead of holding 64 more registers
             float s4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int p = 0; p < P; p++) {
@@ -1113,11 +1122,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
             U[(size_t)(ID2_THREADS + tid) * MAXR + r] = dot;
             if (s2 > bv) { bv = s2; bi = ID2_THREADS + tid; }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-        }
+        warp_argmax(bv, bi);
         buf ^= 1;
         if (lane == 0) { s_bv[buf][wid] = bv; s_bi[buf][wid] = bi; }
         r++;
@@ -1125,8 +1130,8 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     }
     __syncthreads();
     // skeleton and rank; R11 from the pivot rows' dot products (column jj: its entries k < jj)
-    if (pos >= 0) skel[(size_t)t * MAXR + pos] = x;
-    if (xpos >= 0) skel[(size_t)t * MAXR + xpos] = xx;
+    if (pos >= 0) skel[(size_t)t * MAXR + pos] = sxy[tid];
+    if (xpos >= 0) skel[(size_t)t * MAXR + xpos] = sxy[ID2_THREADS + tid];
     if (tid == 0) g.rank[t] = r;
     for (int idx = tid; idx < r * r; idx += ID2_THREADS) {
         const int jj = idx / r, k = idx % r;
@@ -1137,12 +1142,13 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
                                                                  : U[(size_t)pr * MAXR + k]);
     }
     __syncthreads();
-    // back substitution of the non-pivot rows
+    // back substitution of the non-pivot rows, column by column (independent updates)
     if (pos == -1) {
         for (int k = r - 1; k >= 0; k--) {
-            float acc = drow[k];
-            for (int jj = k + 1; jj < r; jj++) acc = fmaf(-R11[jj * (jj + 1) / 2 + k], drow[jj], acc);
-            drow[k] = acc / R11[k * (k + 1) / 2 + k];
+            const float *col = R11 + k * (k + 1) / 2;
+            const float uk = drow[k] / col[k];
+            drow[k] = uk;
+            for (int i = 0; i < k; i++) drow[i] = fmaf(-col[i], uk, drow[i]);
         }
     }
     if (xpos == -1) {

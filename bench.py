@@ -174,22 +174,29 @@ def ours(args, rank, world, local):
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         Pc = scipy_csr_to_c_sparse_matrix(P, lib)
+        w1 = time.perf_counter()
         ws = lib.tsne_init_with_P(None, n, 0, 2, ctypes.byref(prm), Pc)
         if not ws:
             raise RuntimeError("tsne_init_with_P returned NULL")
+        w2 = time.perf_counter()
         rc = lib.tsne_run(ws)
         if rc != 0:
             raise RuntimeError(f"tsne_run failed ({rc})")
+        w3 = time.perf_counter()
         lib.tsne_get_embedding(ws, Yout)
         kl = float(lib.compute_kl_divergence(ws))
+        w4 = time.perf_counter()
         run_ms, attr_ms, attr_n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         lib.tsne_get_timing(ws, ctypes.byref(run_ms), ctypes.byref(attr_ms), ctypes.byref(attr_n))
         nr, nl = ctypes.c_int(), ctypes.c_longlong()
         lib.tsne_get_run_stats(ws, ctypes.byref(nr), ctypes.byref(nl))
         lib.tsne_destroy(ws)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - w0
-        return wall, run_ms.value / 1e3, attr_ms.value, attr_n.value, nl.value, nr.value, kl
+        w5 = time.perf_counter()
+        wall = w5 - w0
+        parts = {"host_P": w1 - w0, "init_with_P": w2 - w1, "run": w3 - w2, "get_embedding_kl": w4 - w3,
+                 "destroy": w5 - w4}
+        return wall, run_ms.value / 1e3, attr_ms.value, attr_n.value, nl.value, nr.value, kl, parts
 
     for _ in range(args.warmup):
         step()
@@ -245,7 +252,8 @@ def ours(args, rank, world, local):
                          "avg_launch_ms": round(attr_ms, 4), "algorithmic_bytes": attr_bytes,
                          "peak_source": peak_src},
             "e2e": {"value": round(wall_s, 4), "unit": "s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h),
+                    "breakdown_s": {k: round(float(np.mean([r[7][k] for r in res])), 4) for k in res[0][7]}},
             "gpu_launches": launches,
             "kl_divergence": round(kl, 5),
             "n_rebuild": res[-1][5],

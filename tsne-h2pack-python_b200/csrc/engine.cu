@@ -1,6 +1,10 @@
 // The optimisation engine behind the C ABI (include/tsne_h2pack.h): one workspace per
 // embedding, all state resident on the current CUDA device, the reference's schedule
 // (src/tsne_h2pack.c:1652-2102) driven from the host with one stream per workspace.
+#include <cstring>
+#include <thread>
+#include <mutex>
+#include <sys/mman.h>
 #include <cub/cub.cuh>
 
 #include <math.h>
@@ -44,7 +48,7 @@ __global__ void k_pad_len(int n, const int *__restrict__ rp, int *__restrict__ l
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         len[i] = (rp[i + 1] - rp[i] + 3) & ~3;
 }
-__global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ pv,
+__global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restrict__ ci, const float *__restrict__ pv,
                            const int *__restrict__ rpp, int *__restrict__ col, float *__restrict__ val)
 {
     const int lane = threadIdx.x & 31;
@@ -53,7 +57,7 @@ __global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restr
         const int b = rp[i], len = rp[i + 1] - b, o = rpp[i], plen = rpp[i + 1] - o;
         for (int e = lane; e < plen; e += 32) {
             col[o + e] = e < len ? ci[b + e] : i;
-            val[o + e] = e < len ? (float)pv[b + e] : 0.f;
+            val[o + e] = e < len ? pv[b + e] : 0.f;
         }
     }
 }
@@ -80,6 +84,24 @@ __global__ void k_conv_check(int n, const float *__restrict__ Y, const float *__
 }
 
 }  // namespace
+
+namespace tsne {
+void keep_pool_memory()
+{
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long keep = ~0ULL;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done[dev] = true;
+}
+}  // namespace tsne
 
 struct tsne_workspace {
     tsne_params_t params{};
@@ -124,20 +146,79 @@ namespace {
 
 template <int D> size_t vec_bytes() { return sizeof(typename Dim<D>::vec); }
 
+// Host staging of P's upload: two pinned buffers (process-wide, one upload at a time) are
+// filled by host threads with a chunk of column indices and values rounded to float (the
+// rounding the device applies), while the previous chunk is copied to the device. This sends
+// 8 bytes per entry at DMA speed instead of 12 bytes per entry through the driver's pageable
+// path.
+struct PinnedStage {
+    std::mutex mu;
+    int *col[2] = {nullptr, nullptr};
+    float *val[2] = {nullptr, nullptr};
+    size_t cap = 0;   // entries per buffer
+};
+PinnedStage &pinned_stage()
+{
+    static PinnedStage s;
+    return s;
+}
+
+void fill_chunk(const int *ci, const double *pv, size_t count, int *col, float *val)
+{
+    const size_t per = size_t(1) << 20;
+    const int nth = (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)std::max(1u, std::thread::hardware_concurrency()),
+                                                             (count + per - 1) / per}));
+    auto work = [&](int k) {
+        const size_t b = count * k / nth, e = count * (k + 1) / nth;
+        memcpy(col + b, ci + b, sizeof(int) * (e - b));
+        for (size_t i = b; i < e; i++) val[i] = (float)pv[i];
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < nth; k++) th.emplace_back(work, k);
+    work(0);
+    for (auto &t : th) t.join();
+}
+
 void upload_P(tsne_workspace *ws)
 {
     const int n = ws->n, nnz = ws->P->row_ptr[n];
     cudaStream_t st = ws->st;
     DevBuf<int> rp0, ci0;
-    DevBuf<double> pv0;
+    DevBuf<float> pv0;
     rp0.exact(n + 1);
     ci0.exact(std::max(nnz, 1));
     pv0.exact(std::max(nnz, 1));
+    const bool tm = env_int("TSNE_E2E_TIMERS", 0) != 0;
+    double t0 = wall_sec();
     TSNE_CUDA_CHECK(cudaMemcpyAsync(rp0.p, ws->P->row_ptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
     if (nnz > 0) {
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(ci0.p, ws->P->col_idx, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(pv0.p, ws->P->values, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+        PinnedStage &ps = pinned_stage();
+        std::lock_guard<std::mutex> lock(ps.mu);
+        constexpr size_t CHUNK = size_t(8) << 20;   // entries per staging buffer
+        if (ps.cap < CHUNK) {
+            for (int b = 0; b < 2; b++) {
+                TSNE_CUDA_CHECK(cudaHostAlloc(&ps.col[b], sizeof(int) * CHUNK, cudaHostAllocPortable));
+                TSNE_CUDA_CHECK(cudaHostAlloc(&ps.val[b], sizeof(float) * CHUNK, cudaHostAllocPortable));
+            }
+            ps.cap = CHUNK;
+        }
+        cudaEvent_t ev[2];
+        for (int b = 0; b < 2; b++) TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+        size_t i = 0;
+        for (size_t c0 = 0; c0 < (size_t)nnz; c0 += CHUNK, i++) {
+            const int b = (int)(i & 1);
+            if (i >= 2) TSNE_CUDA_CHECK(cudaEventSynchronize(ev[b]));
+            const size_t cnt = std::min(CHUNK, (size_t)nnz - c0);
+            fill_chunk(ws->P->col_idx + c0, ws->P->values + c0, cnt, ps.col[b], ps.val[b]);
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(ci0.p + c0, ps.col[b], sizeof(int) * cnt, cudaMemcpyHostToDevice, st));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(pv0.p + c0, ps.val[b], sizeof(float) * cnt, cudaMemcpyHostToDevice, st));
+            TSNE_CUDA_CHECK(cudaEventRecord(ev[b], st));
+        }
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (int b = 0; b < 2; b++) cudaEventDestroy(ev[b]);
     }
+    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (tm) printf("E2E upload_P: alloc + copies %.1f ms\n", 1e3 * (wall_sec() - t0));
     ws->len.exact(n + 1);
     ws->rp.exact(n + 2);
     k_pad_len<<<ceil_div(n, 256), 256, 0, st>>>(n, rp0.p, ws->len.p);
@@ -248,21 +329,19 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     ws->col2.exact(std::max<long long>(nnz, 4));
     ws->val2.exact(std::max<long long>(nnz, 4));
     launch_row_gather(st, n, ord_dev, ws->inv.p, ws->rp.p, ws->col.p, ws->val.p, ws->rp2.p, ws->col2.p, ws->val2.p);
-    std::swap(ws->rp.p, ws->rp2.p); std::swap(ws->rp.cap, ws->rp2.cap);
-    std::swap(ws->col.p, ws->col2.p); std::swap(ws->col.cap, ws->col2.cap);
-    std::swap(ws->val.p, ws->val2.p); std::swap(ws->val.cap, ws->val2.cap);
+    ws->rp.swap(ws->rp2);
+    ws->col.swap(ws->col2);
+    ws->val.swap(ws->val2);
     ws->tmpv.exact(ws->vbytes * n);
     DevBuf<unsigned char> *arrs[] = {&ws->Y, &ws->uY, &ws->gains, &ws->rep, ws->Yconv.p ? &ws->Yconv : nullptr};
     for (DevBuf<unsigned char> *a : arrs) {
         if (a == nullptr) continue;
         launch_permute_vec<D>(st, n, ord_dev, a->p, ws->tmpv.p);
-        std::swap(a->p, ws->tmpv.p);
-        std::swap(a->cap, ws->tmpv.cap);
+        a->swap(ws->tmpv);
     }
     ws->order2.exact(n);
     launch_permute_int(st, n, ord_dev, ws->has_order ? ws->order.p : nullptr, ws->order2.p, ws->has_order ? 0 : 1);
-    std::swap(ws->order.p, ws->order2.p);
-    std::swap(ws->order.cap, ws->order2.cap);
+    ws->order.swap(ws->order2);
     ws->has_order = true;
     ws->n_launch += 11;
 }
@@ -542,6 +621,23 @@ tsne_params_t tsne_create_default_params(void)
     return p;
 }
 
+// Host arrays of a sparse matrix: large ones on 2 MB boundaries with transparent huge pages
+// requested, so that filling (first touch) and freeing a matrix of 10^8 entries takes a few
+// hundred page faults instead of hundreds of thousands. Freed with free().
+static void *host_array(size_t bytes)
+{
+    constexpr size_t HUGE_PAGE = size_t(2) << 20;
+    if (bytes >= HUGE_PAGE) {
+        const size_t rounded = (bytes + HUGE_PAGE - 1) / HUGE_PAGE * HUGE_PAGE;
+        void *p = nullptr;
+        if (posix_memalign(&p, HUGE_PAGE, rounded) == 0) {
+            madvise(p, rounded, MADV_HUGEPAGE);
+            return p;
+        }
+    }
+    return malloc(bytes > 0 ? bytes : 1);
+}
+
 sparse_matrix_t *sparse_matrix_create(int n_rows, int n_cols, int nnz)
 {
     if (n_rows < 0 || nnz < 0) return nullptr;
@@ -550,9 +646,9 @@ sparse_matrix_t *sparse_matrix_create(int n_rows, int n_cols, int nnz)
     m->n_rows = n_rows;
     m->n_cols = n_cols;
     m->nnz = nnz;
-    m->row_ptr = (int *)malloc(sizeof(int) * ((size_t)n_rows + 1));
-    m->col_idx = (int *)malloc(sizeof(int) * ((size_t)nnz > 0 ? nnz : 1));
-    m->values = (double *)malloc(sizeof(double) * ((size_t)nnz > 0 ? nnz : 1));
+    m->row_ptr = (int *)host_array(sizeof(int) * ((size_t)n_rows + 1));
+    m->col_idx = (int *)host_array(sizeof(int) * ((size_t)nnz > 0 ? nnz : 1));
+    m->values = (double *)host_array(sizeof(double) * ((size_t)nnz > 0 ? nnz : 1));
     if (!m->row_ptr || !m->col_idx || !m->values) { sparse_matrix_destroy(m); return nullptr; }
     return m;
 }
@@ -658,6 +754,7 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         ws->vbytes = low_dim == 2 ? vec_bytes<2>() : vec_bytes<3>();
         ws->P = P;
         TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&ws->st, cudaStreamNonBlocking));
+        AllocStream guard(ws->st);
         const size_t vb = ws->vbytes * n_point;
         ws->Y.exact(vb); ws->Yn.exact(vb); ws->uY.exact(vb); ws->gains.exact(vb); ws->rep.exact(vb);
         TSNE_CUDA_CHECK(cudaMemsetAsync(ws->uY.p, 0, vb, ws->st));
@@ -669,7 +766,11 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         ws->part.exact((size_t)ROW_GRID * 3);
         ws->zpart.exact(148 * 2 * 3);
         ws->klpart.exact(ROW_GRID);
+        const bool tm = env_int("TSNE_E2E_TIMERS", 0) != 0;
+        double t0 = wall_sec();
         upload_P(ws);
+        if (tm) printf("E2E init: upload_P %.1f ms\n", 1e3 * (wall_sec() - t0));
+        t0 = wall_sec();
         std::vector<double> Y0((size_t)n_point * low_dim);
         initialize_embedding(Y0.data(), n_point, low_dim, params->init_method, params->init_Y,
                              (unsigned int)params->random_seed);
@@ -692,6 +793,8 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         if (params->verbose)
             printf("Initializing t-SNE with pre-computed P matrix (n=%d, pt_dim=%d, low_dim=%d)\n", n_point, pt_dim,
                    low_dim);
+        if (tm) printf("E2E init: embedding %.1f ms\n", 1e3 * (wall_sec() - t0));
+        t0 = wall_sec();
         const bool never_h2 = (params->h2_rebuild_freq > 0 ? params->h2_rebuild_freq : 10) > 100000;
         if (n_point >= 2000 && !never_h2) {
             if (rebuild_h2(ws) != 0) {
@@ -701,6 +804,7 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
             }
         }
         TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
+        if (tm) printf("E2E init: first H2 build %.1f ms\n", 1e3 * (wall_sec() - t0));
     } catch (const CudaError &) {
         tsne_destroy(ws);
         return nullptr;
@@ -711,6 +815,7 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
 int tsne_run_range(tsne_workspace_t *ws, int iter_begin, int iter_end)
 {
     if (ws == nullptr) return -1;
+    AllocStream guard(ws->st);
     try {
         const long long l0 = ws->n_launch;
         const int rc = ws->d == 2 ? run_range_impl<2>(ws, iter_begin, iter_end) : run_range_impl<3>(ws, iter_begin, iter_end);
@@ -740,6 +845,7 @@ int tsne_run(tsne_workspace_t *ws)
 void tsne_get_embedding(tsne_workspace_t *ws, double *Y_out)
 {
     if (ws == nullptr || Y_out == nullptr) return;
+    AllocStream guard(ws->st);
     try {
         download_soa(ws, ws->Y.p, Y_out);
     } catch (const CudaError &) {
@@ -755,9 +861,16 @@ double compute_kl_divergence(tsne_workspace_t *ws)
 void tsne_destroy(tsne_workspace_t *ws)
 {
     if (ws == nullptr) return;
+    const bool tm = env_int("TSNE_E2E_TIMERS", 0) != 0;
+    double t0 = wall_sec();
     if (ws->st) cudaStreamSynchronize(ws->st);
+    AllocStream guard(ws->st);
+    double t1 = wall_sec();
     ws->h2.reset();
+    double t2 = wall_sec();
     if (ws->P) sparse_matrix_destroy(ws->P);
+    double t3 = wall_sec();
+    if (tm) printf("E2E destroy: sync %.1f ms, h2 %.1f ms, host P %.1f ms\n", 1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (t3 - t2));
     if (ws->prof) {
         free(ws->prof->knn_time); free(ws->prof->p_construction_time); free(ws->prof->p_matvec_time);
         free(ws->prof->h2_rebuild_time); free(ws->prof->h2_matvec_s_time); free(ws->prof->h2_matvec_v_time);
@@ -765,8 +878,10 @@ void tsne_destroy(tsne_workspace_t *ws)
         free(ws->prof);
     }
     cudaStream_t st = ws->st;
+    t0 = wall_sec();
     delete ws;   // device buffers are released here
     if (st) cudaStreamDestroy(st);
+    if (tm) printf("E2E destroy: workspace buffers %.1f ms\n", 1e3 * (wall_sec() - t0));
 }
 
 int tsne_fit_transform_with_P(const double *X, int n_point, int pt_dim, int low_dim, const tsne_params_t *params,
@@ -868,6 +983,7 @@ double compute_repulsive_forces_h2pack(H2Pack_p h2pack_W, const double *Y, int l
 {
     (void)iter;
     if (ws == nullptr || Y == nullptr || grad == nullptr || low_dim != ws->d || n_point != ws->n) return 1.0;
+    AllocStream guard(ws->st);
     try {
         std::vector<double> F((size_t)n_point * low_dim);
         double Z = 1.0;
@@ -903,6 +1019,7 @@ int update_h2_matrix(tsne_workspace_t *ws, int force_rebuild)
 {
     (void)force_rebuild;
     if (ws == nullptr) return -1;
+    AllocStream guard(ws->st);
     try {
         return rebuild_h2(ws);
     } catch (const CudaError &) {
@@ -1016,6 +1133,7 @@ int tsne_set_embedding(tsne_workspace_t *ws, const double *Y_in)
         std::vector<double> Yc((size_t)ws->n * ws->d);
         if (ws->has_order) {
             std::vector<int> ord(ws->n);
+            TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
             TSNE_CUDA_CHECK(cudaMemcpy(ord.data(), ws->order.p, sizeof(int) * ws->n, cudaMemcpyDeviceToHost));
             for (int k = 0; k < ws->d; k++)
                 for (int j = 0; j < ws->n; j++) Yc[(size_t)k * ws->n + j] = Y_in[(size_t)k * ws->n + ord[j]];

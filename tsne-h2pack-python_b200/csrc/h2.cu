@@ -1854,6 +1854,7 @@ public:
     {
         if (!rank_stats_valid_ && built_) {
             std::vector<int> r(n_node_);
+            cudaStreamSynchronize(st_);
             cudaMemcpy(r.data(), rank_.p, sizeof(int) * n_node_, cudaMemcpyDeviceToHost);
             int mx = 0; double sum = 0; int cnt = 0;
             for (int x : r) if (x > 0) { mx = std::max(mx, x); sum += x; cnt++; }

@@ -7,6 +7,7 @@ looks (tsne_h2pack/_lib/, then build/lib/); there is no fallback: a missing libr
 missing CUDA device raises RuntimeError.
 """
 import ctypes
+import os
 import platform
 import sys
 import time
@@ -352,6 +353,26 @@ def scipy_csr_to_sparse_matrix(P_scipy) -> Tuple[SparseMatrix, dict]:
     return m, arrays
 
 
+_copy_pool = None
+
+
+def _copy(dst, src, nbytes, chunk=64 << 20):
+    """memmove of a large host array in chunks on a few threads (ctypes releases the GIL during
+    the copy), so that filling a C matrix of 10^8 entries is not bound by one core."""
+    global _copy_pool
+    if nbytes < 4 * chunk:
+        ctypes.memmove(dst, src, nbytes)
+        return
+    if _copy_pool is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _copy_pool = ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1))
+    dst, src = ctypes.cast(dst, ctypes.c_void_p).value, ctypes.cast(src, ctypes.c_void_p).value
+    jobs = [_copy_pool.submit(ctypes.memmove, dst + o, src + o, min(chunk, nbytes - o))
+            for o in range(0, nbytes, chunk)]
+    for j in jobs:
+        j.result()
+
+
 def scipy_csr_to_c_sparse_matrix(P_scipy, lib) -> "ctypes.POINTER(SparseMatrix)":
     """A C-allocated copy (sparse_matrix_create) that tsne_init_with_P may take over."""
     from scipy.sparse import csr_matrix
@@ -365,10 +386,10 @@ def scipy_csr_to_c_sparse_matrix(P_scipy, lib) -> "ctypes.POINTER(SparseMatrix)"
     rp = np.ascontiguousarray(P_scipy.indptr, dtype=np.int32)
     ci = np.ascontiguousarray(P_scipy.indices, dtype=np.int32)
     pv = np.ascontiguousarray(P_scipy.data, dtype=np.float64)
-    ctypes.memmove(m.row_ptr, rp.ctypes.data, rp.nbytes)
+    _copy(m.row_ptr, rp.ctypes.data, rp.nbytes)
     if P_scipy.nnz:
-        ctypes.memmove(m.col_idx, ci.ctypes.data, ci.nbytes)
-        ctypes.memmove(m.values, pv.ctypes.data, pv.nbytes)
+        _copy(m.col_idx, ci.ctypes.data, ci.nbytes)
+        _copy(m.values, pv.ctypes.data, pv.nbytes)
     return ptr
 
 

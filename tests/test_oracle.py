@@ -25,13 +25,16 @@ def test_init_embedding_equals_reference():
 
 
 def test_engine_init_embedding_equals_oracle():
-    """The engine's initialize_embedding is host code: bit-identical to the oracle's."""
+    """The engine's initialize_embedding is host code with its own copy of the C library's
+    rand() sequence: bit-identical to the oracle's, which calls srand/rand (seeds with the top
+    bit set included, an odd number of values, 3D)."""
     import ctypes
     from tsne_h2pack._backend import get_backend
     lib = get_backend()._lib
     lib.initialize_embedding.argtypes = [np.ctypeslib.ndpointer(np.float64), ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_uint]
-    for n, d, seed in ((1000, 2, 42), (777, 3, 0)):
+    for n, d, seed in ((1000, 2, 42), (777, 3, 0), (100001, 2, 3000000000), (300000, 3, 2**32 - 1), (7, 3, 1),
+                       (64, 2, 2**31)):
         Y = np.zeros((d, n))
         lib.initialize_embedding(Y, n, d, 0, None, seed)
         np.testing.assert_array_equal(Y, O.init_embedding(n, d, seed))

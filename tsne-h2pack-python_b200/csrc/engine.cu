@@ -671,6 +671,30 @@ void sparse_matvec(const sparse_matrix_t *A, const double *x, double *y)
     }
 }
 
+// The C library's rand() sequence after srand(seed), generated without the library's global,
+// locked state: the glibc generator is the additive lagged-Fibonacci generator
+// r[i] = r[i-3] + r[i-31] (mod 2^32), seeded by the Park-Miller LCG (16807, 2^31 - 1) in
+// Schrage's form, with the first 310 outputs discarded; rand() returns r >> 1.
+static void libc_rand_sequence(unsigned int seed, size_t count, unsigned int *out)
+{
+    int32_t r[34];
+    int32_t word = (int32_t)seed;
+    if (word == 0) word = 1;
+    r[0] = word;
+    for (int i = 1; i < 31; i++) {
+        const long hi = word / 127773, lo = word % 127773;
+        long w = 16807 * lo - 2836 * hi;
+        if (w < 0) w += 2147483647;
+        word = (int32_t)w;
+        r[i] = word;
+    }
+    std::vector<uint32_t> ring(34 + 310 + count);
+    for (int i = 0; i < 31; i++) ring[i] = (uint32_t)r[i];
+    for (int i = 31; i < 34; i++) ring[i] = ring[i - 31];
+    for (size_t i = 34; i < ring.size(); i++) ring[i] = ring[i - 31] + ring[i - 3];
+    for (size_t k = 0; k < count; k++) out[k] = ring[k + 344] >> 1;
+}
+
 void initialize_embedding(double *Y, int n_point, int low_dim, int method, const double *Y0, unsigned int seed)
 {
     if (method == 1 && Y0 != nullptr) {
@@ -678,17 +702,30 @@ void initialize_embedding(double *Y, int n_point, int low_dim, int method, const
         return;
     }
     if (method == 1) printf("Warning: init_method=1 without init_Y, using random initialization\n");
-    // N(0, 1e-4^2) by Box-Muller on the C library's rand(), the reference's generator
-    srand(seed);
-    const long total = (long)n_point * low_dim;
-    for (long i = 0; i < total; i += 2) {
-        double u1 = (double)rand() / RAND_MAX;
-        double u2 = (double)rand() / RAND_MAX;
-        if (u1 < 1e-10) u1 = 1e-10;
-        const double rad = sqrt(-2.0 * log(u1));
-        Y[i] = 1e-4 * (rad * cos(2.0 * M_PI * u2));
-        if (i + 1 < total) Y[i + 1] = 1e-4 * (rad * sin(2.0 * M_PI * u2));
-    }
+    // N(0, 1e-4^2) by Box-Muller on the C library's rand() sequence (the reference's generator);
+    // the uniforms are drawn in order, the transform runs on several threads
+    const size_t total = (size_t)n_point * low_dim;
+    const size_t pairs = (total + 1) / 2;
+    std::vector<unsigned int> u(2 * pairs);
+    libc_rand_sequence(seed, u.size(), u.data());
+    const int nth = (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)std::max(1u, std::thread::hardware_concurrency()),
+                                                             pairs / 65536 + 1}));
+    auto work = [&](int k) {
+        const size_t b = pairs * k / nth, e = pairs * (k + 1) / nth;
+        for (size_t p = b; p < e; p++) {
+            double u1 = (double)u[2 * p] / RAND_MAX;
+            const double u2 = (double)u[2 * p + 1] / RAND_MAX;
+            if (u1 < 1e-10) u1 = 1e-10;
+            const double rad = sqrt(-2.0 * log(u1));
+            const size_t i = 2 * p;
+            Y[i] = 1e-4 * (rad * cos(2.0 * M_PI * u2));
+            if (i + 1 < total) Y[i + 1] = 1e-4 * (rad * sin(2.0 * M_PI * u2));
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < nth; k++) th.emplace_back(work, k);
+    work(0);
+    for (auto &t : th) t.join();
 }
 
 sparse_matrix_t *compute_P_from_knn_distances(const double *knn_distances, const int *knn_indices,

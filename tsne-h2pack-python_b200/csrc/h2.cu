@@ -648,10 +648,12 @@ __global__ void __launch_bounds__(128) k_lists_write(int n_node, TreeView tv, Li
 
 // rows of each node's interpolation matrix: a leaf's points, or (upper bound) the
 // children's skeletons; nodes above MIN_ADM_LEVEL are not compressed
-// iflag / lflag: 1 for the internal nodes / leaves at level >= MIN_ADM_LEVEL (the items of
-// the basis launches)
+// iflag / lflag / bflag: 1 for the internal nodes / leaves of at most LEAF_SMALL points / larger
+// leaves at level >= MIN_ADM_LEVEL (the items of the basis launches)
+constexpr int LEAF_SMALL = 64;
 template <int D>
-__global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap, int *__restrict__ iflag, int *__restrict__ lflag)
+__global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap, int *__restrict__ iflag, int *__restrict__ lflag,
+                         int *__restrict__ bflag)
 {
     constexpr int NCH = 1 << D;
     const int n_node = tv.info->n_node;
@@ -661,9 +663,10 @@ __global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap, int *__restrict_
         if (adm) r = tv.leaf[t] ? tv.end[t] - tv.start[t] : NCH * Dim<D>::MAXR;
         rowcap[t] = r;
         iflag[t] = adm && !tv.leaf[t];
-        lflag[t] = adm && tv.leaf[t];
+        lflag[t] = adm && tv.leaf[t] && r <= LEAF_SMALL;
+        bflag[t] = adm && tv.leaf[t] && r > LEAF_SMALL;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) { rowcap[n_node] = 0; iflag[n_node] = 0; lflag[n_node] = 0; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { rowcap[n_node] = 0; iflag[n_node] = 0; lflag[n_node] = 0; bflag[n_node] = 0; }
 }
 
 // ids of the flagged nodes in increasing order
@@ -937,39 +940,44 @@ __device__ __forceinline__ void warp_argmax(float &bv, int &bi)
     bv = __int_as_float(mx);
 }
 
-// Interpolative decompositions of the 2D nodes at level >= 2, one CTA of 128 threads per node,
-// thread `tid` owning candidate row tid (its row of A = K(candidate - c, proxies) in
-// registers). LEAVES: every leaf (candidates = its points; at most 128). Otherwise every
+// Interpolative decompositions of the 2D nodes at level >= 2, one CTA of THREADS threads per
+// node, thread `tid` owning candidate row tid (its row of A = K(candidate - c, proxies) in
+// registers). LEAVES: every leaf (candidates = its points; CTAs of 64 threads for leaves of at
+// most 64 points, which fit seven to an SM, and of 128 for the others). Otherwise every
 // internal node in one dependency-ordered launch (candidates = the children's skeletons):
 // items in decreasing node id (deepest level first), so a node's internal children come
 // before it; it waits for their flags and reads their ranks, skeletons and coefficients
-// through L2. When the children's ranks add up to more than 128, thread tid also owns row
-// 128 + tid, kept in global memory (in the node's first U rows, unused until the end).
+// through L2 (CTAs of 128 threads). When the children's ranks add up to more than 128, thread
+// tid also owns row 128 + tid, kept in global memory (in the node's first U rows, unused until
+// the end).
 // Column-pivoted Gram-Schmidt until the largest residual row norm is <= tol * the largest
 // initial one (ties: the lower row); the dot products of every step are kept in shared
 // memory (row-major, stride MAXR + 1), R11 is gathered from the pivot rows into shared
 // memory, and the back substitution U = [I ; R11^-1 R12]^T runs there. Then U goes out to
 // global memory, with the skeleton and the rank, and the upward coefficients
 // y0 = U^T (the leaf's [1 | x] | the children's y0) are summed by all threads in a fixed order.
-constexpr int ID2_THREADS = 128;
-constexpr int ID2_MAX_ROWS = 2 * ID2_THREADS;   // four children of rank MAXR
+constexpr int ID2_THREADS = 128;                  // internal nodes and leaves of 65..128 points
+constexpr int ID2_SMALL = 64;                     // leaves of at most 64 points
+constexpr int ID2_MAX_ROWS = 2 * ID2_THREADS;     // four children of rank MAXR
 constexpr int ID2_DSTRIDE = Dim<2>::MAXR + 1;
-constexpr size_t ID2_SMEM = sizeof(float) * ID2_THREADS * ID2_DSTRIDE;   // dot products
+constexpr size_t id2_smem(int threads) { return sizeof(float) * threads * ID2_DSTRIDE; }   // dot products
 
-template <bool LEAVES>
-__global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
+template <bool LEAVES, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == ID2_SMALL ? 7 : 4)
+k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
 {
-    constexpr int P = Dim<2>::NPROXY, MAXR = Dim<2>::MAXR, NW = ID2_THREADS / 32;
-    static_assert(ID2_MAX_ROWS >= 4 * MAXR && P == MAXR, "overflow rows reuse U rows of MAXR floats");
-    extern __shared__ float dots[];            // [ID2_THREADS][ID2_DSTRIDE]
+    constexpr int P = Dim<2>::NPROXY, MAXR = Dim<2>::MAXR, NW = THREADS / 32;
+    constexpr int ROWS = LEAVES ? THREADS : 2 * THREADS;   // candidate rows a CTA can hold
+    static_assert(LEAVES || (ROWS >= 4 * MAXR && P == MAXR), "overflow rows reuse U rows of MAXR floats");
+    extern __shared__ float dots[];            // [THREADS][ID2_DSTRIDE]
     __shared__ float prox[P * 2];
     __shared__ float qsh[P];
     __shared__ float rdiag[MAXR];
     __shared__ int piv[MAXR];
     __shared__ float R11[MAXR * (MAXR + 1) / 2];   // column jj at jj (jj + 1) / 2
-    __shared__ float4 sin_[LEAVES ? ID2_THREADS : ID2_MAX_ROWS];
-    __shared__ float4 part[ID2_THREADS];
-    __shared__ float2 sxy[ID2_MAX_ROWS];
+    __shared__ float4 sin_[ROWS];
+    __shared__ float4 part[THREADS];
+    __shared__ float2 sxy[ROWS];
     __shared__ float s_bv[2][NW];
     __shared__ int s_bi[2][NW];
     __shared__ float s_lmax[NW];
@@ -997,12 +1005,12 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     const long long roff = g.rowoff[t];
     float *U = g.U + roff * MAXR;
     const double h = tv.info->radius / (double)(1LL << lvl);
-    for (int p = tid; p < P; p += ID2_THREADS) proxy_point<2>(p, h, prox + p * 2);
+    for (int p = tid; p < P; p += THREADS) proxy_point<2>(p, h, prox + p * 2);
     const float cx = (float)(tv.info->corner[0] + (double)(2 * tv.ix[(size_t)t * 3 + 0] + 1) * h);
     const float cy = (float)(tv.info->corner[1] + (double)(2 * tv.ix[(size_t)t * 3 + 1] + 1) * h);
     // candidates and the upward-pass inputs
     for (int q = 0; q < 2; q++) {
-        const int a = tid + ID2_THREADS * q;
+        const int a = tid + THREADS * q;
         if (a >= m) break;
         float2 pt;
         if (LEAVES) {
@@ -1019,8 +1027,8 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     __syncthreads();
 
     const bool valid = tid < m;
-    const bool big = !LEAVES && m > ID2_THREADS;   // uniform over the block
-    const bool xvalid = big && ID2_THREADS + tid < m;
+    const bool big = !LEAVES && m > THREADS;   // uniform over the block
+    const bool xvalid = big && THREADS + tid < m;
     float row[P];
     int pos = valid ? -1 : -2, xpos = xvalid ? -1 : -2;
     float nrm = -1.f, xnrm = -1.f, lmax = 0.f;
@@ -1040,7 +1048,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     }
     float *xr = U + (size_t)tid * MAXR;   // overflow row, in the node's first U rows
     if (xvalid) {
-        const float2 xx = sxy[ID2_THREADS + tid];
+        const float2 xx = sxy[THREADS + tid];
         const float qx = xx.x - cx, qy = xx.y - cy;
         float z2 = 0.f;
         for (int p = 0; p < P; p++) {
@@ -1054,7 +1062,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     }
     float bv = nrm;
     int bi = valid ? tid : INT_MAX;
-    if (xnrm > bv) { bv = xnrm; bi = ID2_THREADS + tid; }
+    if (xnrm > bv) { bv = xnrm; bi = THREADS + tid; }
     lmax = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(lmax)));
     warp_argmax(bv, bi);
     if (lane == 0) { s_lmax[wid] = lmax; s_bv[0][wid] = bv; s_bi[0][wid] = bi; }
@@ -1080,7 +1088,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
             piv[r] = best;
             pos = r;
             nrm = -1.f;
-        } else if (best == ID2_THREADS + tid) {
+        } else if (best == THREADS + tid) {
             const float rr = sqrtf(xnrm);
             const float inv = 1.0f / rr;
             for (int p = 0; p < P; p++) qsh[p] = xr[p] * inv;
@@ -1119,8 +1127,8 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
                 s2 = fmaf(y, y, s2);
             }
             xnrm = s2;
-            U[(size_t)(ID2_THREADS + tid) * MAXR + r] = dot;
-            if (s2 > bv) { bv = s2; bi = ID2_THREADS + tid; }
+            U[(size_t)(THREADS + tid) * MAXR + r] = dot;
+            if (s2 > bv) { bv = s2; bi = THREADS + tid; }
         }
         warp_argmax(bv, bi);
         buf ^= 1;
@@ -1131,14 +1139,14 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     __syncthreads();
     // skeleton and rank; R11 from the pivot rows' dot products (column jj: its entries k < jj)
     if (pos >= 0) skel[(size_t)t * MAXR + pos] = sxy[tid];
-    if (xpos >= 0) skel[(size_t)t * MAXR + xpos] = sxy[ID2_THREADS + tid];
+    if (xpos >= 0) skel[(size_t)t * MAXR + xpos] = sxy[THREADS + tid];
     if (tid == 0) g.rank[t] = r;
-    for (int idx = tid; idx < r * r; idx += ID2_THREADS) {
+    for (int idx = tid; idx < r * r; idx += THREADS) {
         const int jj = idx / r, k = idx % r;
         if (k > jj) continue;
         const int pr = piv[jj];
         R11[jj * (jj + 1) / 2 + k] = k == jj ? rdiag[jj]
-                                             : (pr < ID2_THREADS ? dots[(size_t)pr * ID2_DSTRIDE + k]
+                                             : (pr < THREADS ? dots[(size_t)pr * ID2_DSTRIDE + k]
                                                                  : U[(size_t)pr * MAXR + k]);
     }
     __syncthreads();
@@ -1152,7 +1160,7 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
         }
     }
     if (xpos == -1) {
-        float *u = U + (size_t)(ID2_THREADS + tid) * MAXR;
+        float *u = U + (size_t)(THREADS + tid) * MAXR;
         for (int k = r - 1; k >= 0; k--) {
             float acc = u[k];
             for (int jj = k + 1; jj < r; jj++) acc = fmaf(-R11[jj * (jj + 1) / 2 + k], u[jj], acc);
@@ -1164,21 +1172,21 @@ __global__ void __launch_bounds__(ID2_THREADS, 4) k_id2d(int n_item, const int *
     if (pos >= 0)
         for (int k = 0; k < r; k++) drow[k] = k == pos ? 1.f : 0.f;
     if (xpos >= 0)
-        for (int k = 0; k < r; k++) U[(size_t)(ID2_THREADS + tid) * MAXR + k] = k == xpos ? 1.f : 0.f;
+        for (int k = 0; k < r; k++) U[(size_t)(THREADS + tid) * MAXR + k] = k == xpos ? 1.f : 0.f;
     __syncthreads();
-    // U rows 0 .. min(m, 128) - 1 out of shared memory (over the overflow rows' scratch)
-    const int mm = min(m, ID2_THREADS);
-    for (int idx = tid; idx < mm * r; idx += ID2_THREADS) {
+    // U rows 0 .. min(m, THREADS) - 1 out of shared memory (over the overflow rows' scratch)
+    const int mm = min(m, THREADS);
+    for (int idx = tid; idx < mm * r; idx += THREADS) {
         const int a = idx / r, k = idx % r;
         U[(size_t)a * MAXR + k] = dots[(size_t)a * ID2_DSTRIDE + k];
     }
-    // y0[k] = sum_a U[a][k] in[a]: groups of RG threads over k, C = 128 / RG groups over a
+    // y0[k] = sum_a U[a][k] in[a]: groups of RG threads over k, C = THREADS / RG groups over a
     const int RG = r <= 16 ? 16 : (r <= 32 ? 32 : 64);
-    const int C = ID2_THREADS / RG, kk = tid % RG, cg = tid / RG;
+    const int C = THREADS / RG, kk = tid % RG, cg = tid / RG;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (kk < r) {
         for (int a = cg; a < m; a += C) {
-            const float w = a < ID2_THREADS ? dots[(size_t)a * ID2_DSTRIDE + kk] : U[(size_t)a * MAXR + kk];
+            const float w = a < THREADS ? dots[(size_t)a * ID2_DSTRIDE + kk] : U[(size_t)a * MAXR + kk];
             fma4(acc, w, sin_[a]);
         }
     }
@@ -1618,8 +1626,12 @@ public:
                                              (int)id_smem_bytes<D>(id_mcap())));
         TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)id_smem_bytes<D>(id_mcap())));
-        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ID2_SMEM));
-        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ID2_SMEM));
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<true, ID2_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)id2_smem(ID2_SMALL)));
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<true, ID2_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)id2_smem(ID2_THREADS)));
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<false, ID2_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)id2_smem(ID2_THREADS)));
     }
 
     int build(const void *Y, int leaf_size, double tol) override
@@ -1659,6 +1671,7 @@ public:
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hrows_, rowoff_.p + cap_node_, sizeof(long long), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hint_, ipos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hleaf_, lpos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(&hbig_, bpos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
             const TreeInfo &I = *hinfo_.p;
             if (I.nonfinite) return -1;
@@ -1729,12 +1742,15 @@ public:
             // leaves in one launch, then the internal nodes of every level in one
             // dependency-ordered launch
             DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
-            if (hleaf_ > 0) k_id2d<true><<<hleaf_, ID2_THREADS, ID2_SMEM, st_>>>(hleaf_, llist_.p, il, dp);
+            if (hleaf_ > 0)
+                k_id2d<true, ID2_SMALL><<<hleaf_, ID2_SMALL, id2_smem(ID2_SMALL), st_>>>(hleaf_, llist_.p, il, dp);
+            if (hbig_ > 0)
+                k_id2d<true, ID2_THREADS><<<hbig_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hbig_, blist_.p, il, dp);
             mark_end(t_bases, 2);
             t_bases = mark_begin();
             if (hint_ > 0) {
                 TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
-                k_id2d<false><<<hint_, ID2_THREADS, ID2_SMEM, st_>>>(hint_, ilist_.p, il, dp);
+                k_id2d<false, ID2_THREADS><<<hint_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hint_, ilist_.p, il, dp);
             }
             launches_ += 2;
             mark_end(t_bases, 7);
@@ -1783,15 +1799,18 @@ public:
         launches_ += 2;
         TSNE_CUDA_CHECK(cudaMemsetAsync(iflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(lflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
-        k_rowcap<D><<<148 * 4, 256, 0, st_>>>(view(), rowcap_.p, iflag_.p, lflag_.p);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(bflag_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
+        k_rowcap<D><<<148 * 4, 256, 0, st_>>>(view(), rowcap_.p, iflag_.p, lflag_.p, bflag_.p);
         scan_exclusive(far_cnt_.p, far_ptr_.p, cap_node_);
         scan_exclusive(near_cnt_.p, near_ptr_.p, cap_node_);
         scan_exclusive_ll(rowcap_.p, rowoff_.p, cap_node_);
         scan_exclusive(iflag_.p, ipos_.p, cap_node_);
         scan_exclusive(lflag_.p, lpos_.p, cap_node_);
+        scan_exclusive(bflag_.p, bpos_.p, cap_node_);
         k_flag_list<<<148 * 4, 256, 0, st_>>>(&info_.p->n_node, iflag_.p, ipos_.p, ilist_.p);
         k_flag_list<<<148 * 4, 256, 0, st_>>>(&info_.p->n_node, lflag_.p, lpos_.p, llist_.p);
-        launches_ += 10;
+        k_flag_list<<<148 * 4, 256, 0, st_>>>(&info_.p->n_node, bflag_.p, bpos_.p, blist_.p);
+        launches_ += 12;
     }
 
     void alloc_lists()
@@ -1804,6 +1823,7 @@ public:
         rowcap_.exact(c + 1);
         iflag_.exact(c + 1); ipos_.exact(c + 2); ilist_.exact(c + 1);
         lflag_.exact(c + 1); lpos_.exact(c + 2); llist_.exact(c + 1);
+        bflag_.exact(c + 1); bpos_.exact(c + 2); blist_.exact(c + 1);
         rowoff_.exact(c + 2);
     }
 
@@ -2090,8 +2110,9 @@ private:
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;
     DevBuf<int> rowcap_;
     DevBuf<int> iflag_, ipos_, ilist_;   // internal nodes at level >= 2, in increasing id
-    DevBuf<int> lflag_, lpos_, llist_;   // leaves at level >= 2, in increasing id
-    int hint_ = 0, hleaf_ = 0;
+    DevBuf<int> lflag_, lpos_, llist_;   // leaves at level >= 2 of at most LEAF_SMALL points
+    DevBuf<int> bflag_, bpos_, blist_;   // the larger leaves at level >= 2
+    int hint_ = 0, hleaf_ = 0, hbig_ = 0;
     DevBuf<long long> rowoff_;
     DevBuf<int> rank_;
     DevBuf<Vec<D>> skel_;

@@ -124,17 +124,23 @@ __device__ __forceinline__ void reduce_partials(const double *__restrict__ part,
 // MB of consecutive rows) and every warp has two independent rows, i.e. two streams of P
 // loads and Y gathers, in flight. A half-warp reads 64 entries per step (4 per lane, two
 // 128-bit loads); lanes 1-3 of the half fetch the row's update operands meanwhile.
-template <int D>
+// MODE ATTR_FUSED: the whole step. ATTR_GRAD: only the attractive sums, stored in `attr`
+// (run while the host reads an H2 build's counts). ATTR_UPDATE: the update from the stored
+// sums, with the same rows per thread and the same summation order as ATTR_FUSED, so the
+// two-kernel form gives the same bits as the fused one.
+enum { ATTR_FUSED = 0, ATTR_GRAD = 1, ATTR_UPDATE = 2 };
+
+template <int D, int MODE>
 __global__ void __launch_bounds__(ROW_BLOCK)
 k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
               const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
               Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
-              float exag4, float mom, float lr, double *__restrict__ partials)
+              float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
 {
     const int lane = threadIdx.x & 31, hl = lane & 15;
     const int half = (blockIdx.x * ROW_BLOCK + threadIdx.x) >> 4;
     const int nhalf = (gridDim.x * ROW_BLOCK) >> 4;
-    const int use_rep = (rep != nullptr) ? *rep_flag : 0;
+    const int use_rep = (MODE != ATTR_GRAD && rep != nullptr) ? *rep_flag : 0;
     double acc[D];
     for (int k = 0; k < D; k++) acc[k] = 0.0;
     // both halves of a warp run the same number of rounds, so full-warp shuffles stay legal
@@ -148,24 +154,43 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
             yi = Y[i];
             b = rp[i];
             e = rp[i + 1];
-            if (hl == 1) opnd = uY[i];
-            else if (hl == 2) opnd = gains[i];
-            else if (hl == 3 && use_rep) opnd = rep[i];
+            if (MODE != ATTR_GRAD) {
+                if (hl == 1) opnd = uY[i];
+                else if (hl == 2) opnd = gains[i];
+                else if (hl == 3 && use_rep) opnd = rep[i];
+            }
         }
         float a[D];
 #pragma unroll
         for (int k = 0; k < D; k++) a[k] = 0.f;
-        for (int base = b + 4 * hl; base < e; base += 64) {
-            const int4 c4 = ld_stream_i4(col + base);
-            const float4 p4 = ld_stream_f4(val + base);
-            attr_acc<D>(yi, Y, c4.x, p4.x, a);
-            attr_acc<D>(yi, Y, c4.y, p4.y, a);
-            attr_acc<D>(yi, Y, c4.z, p4.z, a);
-            attr_acc<D>(yi, Y, c4.w, p4.w, a);
-        }
+        if (MODE == ATTR_UPDATE) {
+            if (live && hl == 0) {
+                const Vec<D> s = attr[i];
 #pragma unroll
-        for (int k = 0; k < D; k++)
-            for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+                for (int k = 0; k < D; k++) a[k] = vget(s, k);
+            }
+        } else {
+            for (int base = b + 4 * hl; base < e; base += 64) {
+                const int4 c4 = ld_stream_i4(col + base);
+                const float4 p4 = ld_stream_f4(val + base);
+                attr_acc<D>(yi, Y, c4.x, p4.x, a);
+                attr_acc<D>(yi, Y, c4.y, p4.y, a);
+                attr_acc<D>(yi, Y, c4.z, p4.z, a);
+                attr_acc<D>(yi, Y, c4.w, p4.w, a);
+            }
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+        }
+        if (MODE == ATTR_GRAD) {
+            if (live && hl == 0) {
+                Vec<D> s = vzero<D>();
+#pragma unroll
+                for (int k = 0; k < D; k++) vset(s, k, a[k]);
+                attr[i] = s;
+            }
+            continue;
+        }
         const int src = lane & 16;
         Vec<D> u = vzero<D>(), g = vzero<D>(), r = vzero<D>();
 #pragma unroll
@@ -193,6 +218,7 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
             Yn[i] = yn;
         }
     }
+    if (MODE == ATTR_GRAD) return;
     // lanes 0 and 16 of each warp hold partial sums: fold lane 16 into lane 0
     for (int k = 0; k < D; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
@@ -521,9 +547,26 @@ void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, c
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
                         const int *rep_flag, float exag4, float mom, float lr, double *partials)
 {
-    k_attr_update<D><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+    k_attr_update<D, ATTR_FUSED><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials);
+        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
+}
+template <int D>
+void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
+                      void *attr)
+{
+    k_attr_update<D, ATTR_GRAD><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, 0.f, nullptr,
+        (Vec<D> *)attr);
+}
+template <int D>
+void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Ynext, void *uY, void *gains,
+                   const void *rep, const int *rep_flag, const void *attr, float exag4, float mom, float lr,
+                   double *partials)
+{
+    k_attr_update<D, ATTR_UPDATE><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, nullptr, nullptr, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
 }
 
 template <int D>
@@ -620,6 +663,11 @@ void launch_pcal(cudaStream_t st, int n, const int *indptr, const double *dist, 
     template void launch_attr_update<D>(cudaStream_t, int, const int *, const int *, const float *,  \
                                         const void *, void *, void *, void *, const void *,          \
                                         const int *, float, float, float, double *);                 \
+    template void launch_attr_grad<D>(cudaStream_t, int, const int *, const int *, const float *,    \
+                                      const void *, void *);                                         \
+    template void launch_update<D>(cudaStream_t, int, const int *, const void *, void *, void *,     \
+                                   void *, const void *, const int *, const void *, float, float,    \
+                                   float, double *);                                                 \
     template void launch_center<D>(cudaStream_t, int, const void *, void *, const double *,         \
                                    DevScalars *, const void *, double *);                            \
     template void launch_exact_sv<D>(cudaStream_t, int, const void *, float *, void *);             \

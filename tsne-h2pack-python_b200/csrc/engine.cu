@@ -1,6 +1,7 @@
 // The optimisation engine behind the C ABI (include/tsne_h2pack.h): one workspace per
 // embedding, all state resident on the current CUDA device, the reference's schedule
 // (src/tsne_h2pack.c:1652-2102) driven from the host with one stream per workspace.
+#include <functional>
 #include <cstring>
 #include <thread>
 #include <mutex>
@@ -116,6 +117,7 @@ struct tsne_workspace {
     long long padded_nnz = 0;
     DevBuf<float> val, val2;
     DevBuf<unsigned char> Y, Yn, uY, gains, rep, frc, tmpv, Yconv;
+    DevBuf<unsigned char> attr;     // attractive sums of a rebuild iteration (computed during the build)
     DevBuf<float> s;
     DevBuf<unsigned char> v;
     DevBuf<DevScalars> sc;
@@ -277,14 +279,14 @@ void download_soa(tsne_workspace *ws, const void *src, double *out)
 
 // Rebuild the H2 matrix for the current embedding (reference update_h2_matrix,
 // src/tsne_h2pack.c:772-953). 0 ok (h2_valid tells whether an H2 matrix exists), -1 failure.
-int rebuild_h2(tsne_workspace *ws)
+int rebuild_h2(tsne_workspace *ws, const std::function<void()> *overlap = nullptr)
 {
     if (ws->n < 2000) { ws->h2_valid = false; return 0; }
     if (!ws->h2) ws->h2 = make_h2_matrix(ws->d, ws->n, ws->st);
     const int leaf = ws->params.h2_leaf_size > 0 ? ws->params.h2_leaf_size : 100;
     const double tol = ws->params.h2_tol > 0.0 ? ws->params.h2_tol : 1e-6;
     const long long l0 = ws->h2->launches();
-    const int rc = ws->h2->build(ws->Y.p, leaf, tol);
+    const int rc = ws->h2->build(ws->Y.p, leaf, tol, overlap);
     ws->n_launch += ws->h2->launches() - l0;
     if (rc < 0) {
         fprintf(stderr, "ERROR: Y contains NaN or Inf!\n");
@@ -434,6 +436,7 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
         if (iter >= 20 && iter < p.early_exag_iter && rep_reuse && p.h2_rebuild_freq_early > eff)
             eff = p.h2_rebuild_freq_early;
         bool rebuilt = (iter == 0);
+        bool attr_ready = false;
         const bool want = iter > 0 && iter % eff == 0;
         if (n >= 2000 && want && !never_h2) {
             size_t e0 = evused;
@@ -444,7 +447,15 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
                 renumber(ws, ws->h2->perm_device());
                 if (env_int("TSNE_H2_TIMERS", 0)) printf("RENUMBER iter %d %.1f ms\n", iter, 1e3 * (wall_sec() - t0));
             }
-            if (rebuild_h2(ws) != 0) {
+            // the attractive sums of this iteration depend on Y only: they run while the host
+            // waits for the build's counts
+            const std::function<void()> overlap = [&]() {
+                ws->attr.exact(ws->vbytes * n);
+                launch_attr_grad<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->attr.p);
+                attr_ready = true;
+                ws->n_launch++;
+            };
+            if (rebuild_h2(ws, &overlap) != 0) {
                 fprintf(stderr, "ERROR: Failed to rebuild H2 matrix at iteration %d\n", iter);
                 ret = -1;
                 break;
@@ -495,10 +506,15 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
 
         size_t e2 = evused;
         if (prof) stage_event(ws, evpool, evused);
-        if (ktime) stage_event(ws, kev, kused);
-        launch_attr_update<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p, ws->uY.p, ws->gains.p,
-                              force, flag, (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
-        if (ktime) stage_event(ws, kev, kused);
+        if (attr_ready) {
+            launch_update<D>(st, n, ws->rp.p, ws->Y.p, ws->Yn.p, ws->uY.p, ws->gains.p, force, flag, ws->attr.p,
+                             (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
+        } else {
+            if (ktime) stage_event(ws, kev, kused);
+            launch_attr_update<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p, ws->uY.p, ws->gains.p,
+                                  force, flag, (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
+            if (ktime) stage_event(ws, kev, kused);
+        }
         if (prof) { stage_event(ws, evpool, evused); stages.push_back({iter, 0, e2, evused - 1}); }
         size_t e3 = evused;
         if (prof) stage_event(ws, evpool, evused);

@@ -1599,6 +1599,11 @@ inline int grid_for(long long work, int block, int cap = 148 * 16)
 template <int D>
 class H2Impl final : public H2Matrix {
 public:
+    ~H2Impl() override
+    {
+        if (counts_ev_) cudaEventDestroy(counts_ev_);
+    }
+
     H2Impl(int n, cudaStream_t st) : n_(n), st_(st)
     {
         keys_in_.exact(n); keys_.exact(n); idx_in_.exact(n); perm_.exact(n); xt_.exact(n);
@@ -1612,6 +1617,7 @@ public:
         ticket_.exact(1);
         info_.exact(1);
         TSNE_CUDA_CHECK(cudaMemsetAsync(info_.p, 0, sizeof(TreeInfo), st_));
+        TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&counts_ev_, cudaEventDisableTiming));
         size_t b1 = 0, b2 = 0;
         TSNE_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, b1, keys_in_.p, keys_.p, idx_in_.p,
                                                         perm_.p, n, 0, D * Dim<D>::L, st_));
@@ -1634,7 +1640,7 @@ public:
                                              (int)id2_smem(ID2_THREADS)));
     }
 
-    int build(const void *Y, int leaf_size, double tol) override
+    int build(const void *Y, int leaf_size, double tol, const std::function<void()> *overlap) override
     {
         leaf_size_ = leaf_size;
         const int L = Dim<D>::L;
@@ -1672,7 +1678,12 @@ public:
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hint_, ipos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hleaf_, lpos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(&hbig_, bpos_.p + cap_node_, sizeof(int), cudaMemcpyDeviceToHost, st_));
-            TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+            TSNE_CUDA_CHECK(cudaEventRecord(counts_ev_, st_));
+            if (overlap != nullptr && *overlap) {
+                (*overlap)();
+                overlap = nullptr;
+            }
+            TSNE_CUDA_CHECK(cudaEventSynchronize(counts_ev_));
             const TreeInfo &I = *hinfo_.p;
             if (I.nonfinite) return -1;
             if (I.pad[1]) {   // a dependency wait of the previous build gave up
@@ -2113,6 +2124,7 @@ private:
     DevBuf<int> lflag_, lpos_, llist_;   // leaves at level >= 2 of at most LEAF_SMALL points
     DevBuf<int> bflag_, bpos_, blist_;   // the larger leaves at level >= 2
     int hint_ = 0, hleaf_ = 0, hbig_ = 0;
+    cudaEvent_t counts_ev_ = nullptr;   // end of a build's count batch (host waits on it)
     DevBuf<long long> rowoff_;
     DevBuf<int> rank_;
     DevBuf<Vec<D>> skel_;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -21,8 +22,11 @@ public:
     virtual ~H2Matrix() = default;
     // Build for the points Y (device, point order). Returns 0 on success, -1 when Y holds
     // a non-finite coordinate, 1 when the tree is too shallow for an H2 matrix
-    // (max_level <= 2: the caller uses the exact sums).
-    virtual int build(const void *Y, int leaf_size, double tol) = 0;
+    // (max_level <= 2: the caller uses the exact sums). `overlap`, when given, is called
+    // once, after the tree and list-count kernels are queued and before the host waits for
+    // their counts: work it queues on the stream keeps the GPU busy meanwhile (it must not
+    // depend on the tree).
+    virtual int build(const void *Y, int leaf_size, double tol, const std::function<void()> *overlap = nullptr) = 0;
     // [s | v] = K [1 | Y] - [1 | Y] (diagonal excluded), tree order; then the Z identity and
     // the force, written in point order into F. keep_rep marks F as the stored force.
     virtual void product_force(void *F, DevScalars *sc, double *partials, int keep_rep) = 0;

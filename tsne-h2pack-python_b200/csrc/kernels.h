@@ -39,6 +39,14 @@ template <int D>
 void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
                         const int *rep_flag, float exag4, float mom, float lr, double *partials);
+// the attractive sums alone (into attr), and the update from them (same bits as the fused step)
+template <int D>
+void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
+                      void *attr);
+template <int D>
+void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Ynext, void *uY, void *gains,
+                   const void *rep, const int *rep_flag, const void *attr, float exag4, float mom, float lr,
+                   double *partials);
 template <int D>
 void launch_center(cudaStream_t st, int n, const void *Ynext, void *Ycur, const double *partials,
                    DevScalars *sc, const void *Yprev_conv, double *conv_partials);

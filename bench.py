@@ -66,6 +66,14 @@ def parse():
     ap.add_argument("--save-embedding", default=None)
     ap.add_argument("--graph-cache", default=None, help="npz file holding the k-NN graph and P")
     ap.add_argument("--profile-csv", default=None, help="write the per-iteration stage CSV of the last step")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: the 1M-point run (default); batched: many small embeddings through the "
+                         "job server; served: Poisson arrivals of embedding jobs")
+    ap.add_argument("--jobs", type=int, default=256, help="batched: number of embeddings")
+    ap.add_argument("--rate", type=float, default=2.0, help="served: arrival rate, jobs/s")
+    ap.add_argument("--duration", type=float, default=60.0, help="served: arrival window, seconds")
+    ap.add_argument("--max-concurrent", type=int, default=16)
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     return ap.parse_args()
 
 
@@ -288,6 +296,173 @@ def cpu_sample(P, n, iters):
                       f"{t_rb:.2f} s) + {iters} x pass {t_pass:.3f} s"}
 
 
+def _job_inputs(specs, device, zipf=False):
+    """P of each (n, clusters, perplexity, low_dim, seed, k) job: a 50-dim float32 mixture
+    (equal clusters, centres N(0, 5^2), unit noise; or with zipf, the 1M workload's recipe:
+    100 Zipf(1.1) clusters, centres N(0, 3^2), per-dimension std U(0.5, 2)), exact k-NN graph on
+    the GPU, device calibration (setup, untimed)."""
+    from tsne_h2pack._backend import get_backend
+    from tsne_h2pack._synthetic import knn_graph_torch, mixture_equal, mixture_zipf
+    be = get_backend()
+    out = []
+    for n, c, perp, d, seed, k in specs:
+        if zipf:
+            X, _ = mixture_zipf(n, seed=seed)
+        else:
+            X, _ = mixture_equal(n, n_clusters=c, dim=50, seed=seed, dtype=np.float32)
+        G = knn_graph_torch(X, min(k, n - 1), device=f"cuda:{device}")
+        out.append((be.joint_P(G, perp), d, perp))
+    return out
+
+
+def _job_params(be, n, iters, perp, seed):
+    p = be.create_default_params()
+    p.n_iter = iters
+    p.verbose = 0
+    p.perplexity = perp
+    p.learning_rate = max(n / 12.0, 200.0)
+    p.h2_tol, p.h2_rebuild_freq, p.h2_rebuild_freq_early, p.h2_leaf_size = 1e-2, 3, 10, 100
+    p.random_seed = seed
+    p.init_method = 0
+    return p
+
+
+def _serial_plain(be, inputs, iters):
+    """The same jobs one after another through the plain C ABI path; per-job latency."""
+    from tsne_h2pack._backend import scipy_csr_to_c_sparse_matrix
+    lib = be._lib
+    lat = []
+    for i, (P, d, perp) in enumerate(inputs):
+        n = P.shape[0]
+        t0 = time.perf_counter()
+        prm = _job_params(be, n, iters, perp, i)
+        ws = lib.tsne_init_with_P(None, n, 0, d, ctypes.byref(prm), scipy_csr_to_c_sparse_matrix(P, lib))
+        if not ws or lib.tsne_run(ws) != 0:
+            raise RuntimeError("plain job failed")
+        Y = np.zeros((d, n))
+        lib.tsne_get_embedding(ws, Y)
+        lib.tsne_destroy(ws)
+        lat.append(time.perf_counter() - t0)
+    return lat
+
+
+def _pcts(x):
+    x = np.asarray(x)
+    return {"p50": round(float(np.percentile(x, 50)), 4), "p95": round(float(np.percentile(x, 95)), 4),
+            "p99": round(float(np.percentile(x, 99)), 4)}
+
+
+def batched(args, local):
+    """Batched form: J embeddings, N log-uniform in [2000, 50000], 5-30 equal clusters,
+    perplexity from {10, 30, 50}, k = 3 perplexity, 2D, 750 iterations, all submitted at once
+    to the job server; against the same jobs run one after another (plain path)."""
+    import torch
+    from tsne_h2pack._backend import get_backend
+    from tsne_h2pack.serving import EmbeddingServer
+    torch.cuda.set_device(local)
+    be = get_backend()
+    rng = np.random.default_rng(1234)
+    specs = []
+    for j in range(args.jobs):
+        n = int(round(np.exp(rng.uniform(np.log(2000), np.log(50000)))))
+        perp = float(rng.choice([10.0, 30.0, 50.0]))
+        specs.append((n, int(rng.integers(5, 31)), perp, 2, 1000 + j, int(3 * perp)))
+    iters = 750
+    t0 = time.time()
+    inputs = _job_inputs(specs, local)
+    setup = time.time() - t0
+    for i in range(min(3, len(inputs))):   # warm-up (allocator pool, module load)
+        _serial_plain(be, inputs[i:i + 1], 50)
+    clocks = Clocks(local)
+    clocks.start()
+    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb) as srv:
+        t0 = time.perf_counter()
+        ids = [srv.submit(P, n_components=d, params=_job_params(be, P.shape[0], iters, perp, i))
+               for i, (P, d, perp) in enumerate(inputs)]
+        res = [srv.wait(j)[1] for j in ids]
+        wall = time.perf_counter() - t0
+    ck = clocks.stop()
+    assert all(r.ok for r in res)
+    t1 = time.perf_counter()
+    lat_serial = _serial_plain(be, inputs, iters)
+    wall_serial = time.perf_counter() - t1
+    value = len(inputs) / wall
+    out = {"metric": f"batched jobs/s ({len(inputs)} embeddings, N 2K-50K, {iters} iters, 2D)",
+           "value": round(value, 3), "unit": "jobs/s", "n_gpus": 1, "steps": 1, "warmup": 3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic: equal-cluster 50-dim float32 mixtures, seed 1234; exact k = 3 perplexity graphs",
+           "config": {"workload": "batched", "jobs": len(inputs), "max_concurrent": args.max_concurrent,
+                      "hbm_budget_gb": args.hbm_budget_gb, "iterations": iters,
+                      "n_points_total": int(sum(P.shape[0] for P, _, _ in inputs))},
+           "serial_plain": {"value": round(len(inputs) / wall_serial, 3), "unit": "jobs/s",
+                            "latency_s": _pcts(lat_serial)},
+           "speedup_vs_serial": round(wall_serial / wall, 3),
+           "latency_s": _pcts([r.latency_s for r in res]), "wall_s": round(wall, 3),
+           "setup_s": round(setup, 1)}
+    if ck:
+        out["clocks"] = ck
+    return out
+
+
+def served(args, local):
+    """Served form: Poisson arrivals at `rate` jobs/s for `duration` s; N log-uniform in
+    [5000, 200000], 2D (80%) or 3D (20%), 50-dim float32 Zipf mixtures, k = 90, perplexity 30,
+    1000 iterations; jobs submitted at their arrival times to the job server. Reports jobs/s
+    and p50/p95/p99 latency (arrival to result), and the same jobs run serially."""
+    import torch
+    from tsne_h2pack._backend import get_backend
+    from tsne_h2pack.serving import EmbeddingServer
+    torch.cuda.set_device(local)
+    be = get_backend()
+    rng = np.random.default_rng(4321)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / args.rate)
+        if t > args.duration:
+            break
+        arrivals.append(t)
+    specs = []
+    for j in range(len(arrivals)):
+        n = int(round(np.exp(rng.uniform(np.log(5000), np.log(200000)))))
+        d = 2 if rng.uniform() < 0.8 else 3
+        specs.append((n, int(rng.integers(5, 31)), 30.0, d, 5000 + j, 90))
+    iters = 1000
+    t0 = time.time()
+    inputs = _job_inputs(specs, local, zipf=True)
+    setup = time.time() - t0
+    for i in range(min(2, len(inputs))):
+        _serial_plain(be, inputs[i:i + 1], 50)
+    clocks = Clocks(local)
+    clocks.start()
+    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb) as srv:
+        start = time.perf_counter()
+        ids = []
+        for i, ((P, d, perp), at) in enumerate(zip(inputs, arrivals)):
+            delay = start + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(P, n_components=d, params=_job_params(be, P.shape[0], iters, perp, i)))
+        res = [srv.wait(j)[1] for j in ids]
+        wall = time.perf_counter() - start
+    ck = clocks.stop()
+    assert all(r.ok for r in res)
+    lat_serial = _serial_plain(be, inputs, iters)
+    out = {"metric": f"served jobs/s (Poisson {args.rate}/s for {args.duration:.0f} s, N 5K-200K, {iters} iters)",
+           "value": round(len(inputs) / wall, 3), "unit": "jobs/s", "n_gpus": 1, "steps": 1, "warmup": 2,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic: 50-dim float32 Zipf(1.1) mixtures, seed 4321; exact k = 90 graphs",
+           "config": {"workload": "served", "jobs": len(inputs), "rate": args.rate, "duration_s": args.duration,
+                      "max_concurrent": args.max_concurrent, "hbm_budget_gb": args.hbm_budget_gb,
+                      "iterations": iters},
+           "latency_s": _pcts([r.latency_s for r in res]), "queue_s": _pcts([r.queue_s for r in res]),
+           "serial_plain": {"value": round(len(inputs) / sum(lat_serial), 3), "unit": "jobs/s",
+                            "run_s": _pcts(lat_serial)},
+           "wall_s": round(wall, 3), "setup_s": round(setup, 1)}
+    if ck:
+        out["clocks"] = ck
+    return out
+
+
 def rebuild_count(iters, freq=3, early=10, exag_iter=250):
     c = 1
     for it in range(1, iters):
@@ -330,7 +505,10 @@ def main():
         torch.cuda.set_device(local)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        out = ours(args, rank, world, local) if args.impl == "ours" else reference(args, rank, world, local)
+        if args.workload != "plain":
+            out = (batched if args.workload == "batched" else served)(args, local) if rank == 0 else None
+        else:
+            out = ours(args, rank, world, local) if args.impl == "ours" else reference(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as tdist

@@ -228,6 +228,39 @@ TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, lon
 TSNE_API int tsne_exact_repulsion_static(const float *Y, int n_point, int low_dim, float *F, double *Z,
                                          void *stream);
 
+/* ---- Batched and served jobs (no counterpart in the reference, which runs one embedding
+ * per call). A server runs many independent optimisations on the current device: jobs queue
+ * in arrival order and start when fewer than max_concurrent run and their device memory
+ * estimate fits under hbm_budget_gb next to the running jobs' (a job larger than the budget
+ * runs alone). Each job is a workspace with its own stream, so running jobs overlap on the
+ * GPU; a job's result is the one it gets alone, bit for bit. */
+typedef struct tsne_server tsne_server_t;
+
+typedef struct {
+    int job;            /* id returned by tsne_server_submit */
+    int status;         /* 0: done; -1: failed or cancelled */
+    int n_point, low_dim;
+    double latency_s;   /* submission to completion */
+    double queue_s;     /* submission to start */
+    double run_s;       /* tsne_init_with_P + tsne_run + read-back */
+    double kl;          /* final KL divergence */
+    double start_s, end_s;   /* steady-clock times of start and completion */
+} tsne_job_info_t;
+
+/* NULL on bad arguments or when no CUDA device is current. */
+TSNE_API tsne_server_t *tsne_server_create(int max_concurrent, double hbm_budget_gb);
+/* Queues one job; takes ownership of P (from sparse_matrix_create) as tsne_init_with_P does,
+ * copies params and init_Y. Returns the job id (>= 0) or -1 on bad arguments. */
+TSNE_API int tsne_server_submit(tsne_server_t *s, int n_point, int low_dim, const tsne_params_t *params,
+                                sparse_matrix_t *P);
+/* Blocks until the job ends; Y_out (low_dim x n_point, may be NULL) and info (may be NULL)
+ * receive the result. Returns 0, or -1 when the job failed or was cancelled. */
+TSNE_API int tsne_server_wait(tsne_server_t *s, int job, DTYPE *Y_out, tsne_job_info_t *info);
+/* Jobs queued or running. */
+TSNE_API int tsne_server_pending(tsne_server_t *s);
+/* Cancels the jobs that have not started, waits for the running ones, frees everything. */
+TSNE_API void tsne_server_destroy(tsne_server_t *s);
+
 #ifdef __cplusplus
 }
 #endif

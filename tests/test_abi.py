@@ -105,3 +105,31 @@ def test_device_constants_match_oracle():
     rho = re.search(r"#define ORA_SHELL_RHO_LIST ([0-9., ]+)", ora).group(1)
     assert [float(x) for x in rho.split(",")] == [3.0, 4.5, 7.0, 12.0]
     assert "k == 0 ? 3.0 : k == 1 ? 4.5 : k == 2 ? 7.0 : 12.0" in cu
+
+
+def test_job_info_layout_matches_header(tmp_path):
+    """tsne_job_info_t of the batched/served entry points: ctypes layout = compiled header."""
+    from tsne_h2pack.serving import JobInfo
+    fields = [f for f, _ in JobInfo._fields_]
+    src = tmp_path / "job.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "tsne_h2pack.h"\nint main(void){\n'
+                   + "".join(f'printf("{f} %zu\\n", offsetof(tsne_job_info_t, {f}));\n' for f in fields)
+                   + 'printf("sizeof %zu\\n", sizeof(tsne_job_info_t));\nreturn 0;}\n')
+    exe = tmp_path / "job"
+    subprocess.run(["gcc", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split("\n") if line)
+    for f in fields:
+        assert int(out[f]) == getattr(JobInfo, f).offset, f
+    assert int(out["sizeof"]) == ctypes.sizeof(JobInfo)
+
+
+def test_server_rejects_bad_arguments_without_a_device():
+    """tsne_server_create validates its arguments before touching the device."""
+    from tsne_h2pack.serving import _bind
+    from tsne_h2pack._backend import get_backend
+    lib = get_backend()._lib
+    _bind(lib)
+    assert not lib.tsne_server_create(0, 10.0)
+    assert not lib.tsne_server_create(2, 0.0)
+    assert lib.tsne_server_submit(None, 10, 2, None, None) == -1
+    assert lib.tsne_server_pending(None) == -1

@@ -160,6 +160,40 @@ def test_force_path_matches_general_product(mid, n_iter):
     assert abs(Z - Zg) < 2e-5 * Zg
 
 
+@pytest.fixture(scope="module")
+def evolved3d(mid):
+    """3D embeddings of the mid problem after 20 and 150 iterations of the oracle's run."""
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 3, 6)
+    return P, {it: O.run(P, Y0, n_iter=it)[0].astype(np.float32).astype(np.float64) for it in (20, 150)}
+
+
+@pytest.mark.parametrize("n_iter", [20, 150])
+def test_h2_3d_tree_lists_and_force(evolved3d, n_iter):
+    """3D: tree permutation, node table and lists bit-exact against the oracle; the H2 force
+    (shared-memory ID with grouped rows) within h2_tol of the exact FP64 force."""
+    P, Ys = evolved3d
+    Y = Ys[n_iter]
+    eng = Engine(P, Y, n_iter=1)
+    assert eng.rebuild() == 0
+    dev = eng.h2()
+    h = O.H2(Y, leaf_size=100, tol=1e-2)
+    np.testing.assert_array_equal(h.perm(), dev["perm"])
+    on = h.nodes()
+    for k in on:
+        np.testing.assert_array_equal(on[k], dev["nodes"][k], err_msg=k)
+    fp, fi, np_, ni = h.lists()
+    np.testing.assert_array_equal(fi, dev["far_idx"])
+    np.testing.assert_array_equal(ni, dev["near_idx"])
+    F, Z = eng.repulsive(Y)
+    eng.close()
+    s, v = O.exact_sv(Y)
+    Ze, Fe = O.z_force(Y, s, v)
+    print(f"3D iter {n_iter}: force rel {rel2(F, Fe):.3e}, Z rel {abs(Z - Ze) / Ze:.3e}")
+    assert rel2(F, Fe) <= 1e-2
+    assert abs(Z - Ze) <= 1e-2 * Ze
+
+
 def test_attractive_matches_oracle(mid):
     from tsne_h2pack._backend import scipy_csr_to_c_sparse_matrix
     X, G, P, _ = mid

@@ -39,6 +39,8 @@ namespace {
 template <int D> using Vec = typename Dim<D>::vec;
 
 constexpr int ID_THREADS = 128;
+constexpr int IDG_THREADS = 256;     // shared-memory ID kernel (3D, large 2D leaves)
+constexpr int IDG_GROUP = 4;         // its threads per candidate row in a Gram-Schmidt step
 constexpr int NEAR_THREADS = 128;
 constexpr int STACK_CAP = 192;       // leaf-target descent stack (depth * (2^D - 1) + 2^D)
 
@@ -53,6 +55,13 @@ struct TreeView {
     int *btot;               // |B_l|
     TreeInfo *info;
 };
+
+__device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
+{
+    acc.x = fmaf(w, v.x, acc.x); acc.y = fmaf(w, v.y, acc.y);
+    acc.z = fmaf(w, v.z, acc.z); acc.w = fmaf(w, v.w, acc.w);
+}
+__device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
 
 // ---------------------------------------------------------------------------------
 // root box and keys
@@ -547,8 +556,9 @@ __device__ void process_target(const TreeView &tv, ListOut &lo, int t)
         lo.near_cnt[t] = nc;
         if (ns > tv.nset_cap) { atomicExch(&tv.info->nset_overflow, 1); ns = tv.nset_cap; }
         lo.nset_cnt[t] = ns;
-    } else {
-        // ascending partners (insertion sort of this target's segments)
+    } else if (D == 2) {
+        // ascending partners (insertion sort of this target's short segments; 3D lists are
+        // longer and are sorted afterwards by a segmented sort)
         int *f = lo.far_idx + lo.far_ptr[t];
         for (int a = 1; a < fc; a++) { const int v = f[a]; int z = a - 1; while (z >= 0 && f[z] > v) { f[z + 1] = f[z]; z--; } f[z + 1] = v; }
         int *g = lo.near_idx + lo.near_ptr[t];
@@ -750,16 +760,34 @@ constexpr size_t id_smem_bytes(int mcap)
 // a step produces is stored in the pivot row of A, which no later step reads.
 // LEAVES = true: every leaf at level >= 2 (leaves depend on nothing), blockIdx.x counts
 // from the first node of level 2; false: the internal nodes of one level.
+// items != nullptr: the internal nodes of every level in one dependency-ordered launch (items
+// in increasing node id, taken deepest first; a node waits for its internal children's flags);
+// otherwise the nodes of `level` (or every leaf). Children's ranks, skeletons and coefficients
+// are read through L2.
 template <int D, bool LEAVES>
-__global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
+__global__ void __launch_bounds__(IDG_THREADS) k_id(int level, IdArgs g, int n_item, const int *__restrict__ items,
+                                                    DepArgs dp)
 {
-    constexpr int P = Dim<D>::NPROXY, PP = P + 1, MAXR = Dim<D>::MAXR;
+    constexpr int P = Dim<D>::NPROXY, PP = P + 1, MAXR = Dim<D>::MAXR, NCH = 1 << D;
     extern __shared__ __align__(16) unsigned char smraw[];
     const TreeView &tv = g.tv;
-    const int t = tv.info->level_begin[LEAVES ? MIN_ADM_LEVEL : level] + blockIdx.x;
-    if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) return;
-    const int lvl = tv.level[t];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    __shared__ int s_item;
+    __shared__ int s_coff[NCH + 1];   // children's first candidate row
+    __shared__ float4 s_part[IDG_THREADS];
+    int t;
+    if (items != nullptr) {
+        if (tid == 0) s_item = atomicAdd(dp.ticket, 1);
+        __syncthreads();
+        if (s_item >= n_item) return;
+        t = items[n_item - 1 - s_item];
+        if (!LEAVES && tid < tv.nchild[t] && !tv.leaf[tv.fchild[t] + tid]) dep_wait(dp, tv.fchild[t] + tid);
+        __syncthreads();
+    } else {
+        t = tv.info->level_begin[LEAVES ? MIN_ADM_LEVEL : level] + blockIdx.x;
+        if (LEAVES ? !tv.leaf[t] : tv.leaf[t] != 0) return;
+    }
+    const int lvl = tv.level[t];
     const Vec<D> *xt = (const Vec<D> *)g.xt;
     Vec<D> *skel = (Vec<D> *)g.skel;
 
@@ -771,14 +799,25 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     int *sel = (int *)ptr; ptr += sizeof(int) * MAXR;
     float *A_s = (float *)ptr;
 
-    __shared__ float s_bv[ID_THREADS / 32];
-    __shared__ int s_bi[ID_THREADS / 32];
+    __shared__ float s_bv[IDG_THREADS / 32];
+    __shared__ int s_bi[IDG_THREADS / 32];
     __shared__ int s_best, s_stop;
     __shared__ float s_n0;
 
     int m = 0;
     if (LEAVES) m = tv.end[t] - tv.start[t];
-    else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
+    else {
+        if (tid == 0) {
+            int acc = 0;
+            for (int c = 0; c < tv.nchild[t]; c++) {
+                s_coff[c] = acc;
+                acc += __ldcg(g.rank + tv.fchild[t] + c);
+            }
+            s_coff[tv.nchild[t]] = acc;
+        }
+        __syncthreads();
+        m = s_coff[tv.nchild[t]];
+    }
     const long long roff = g.rowoff[t];
     const bool glob = m > g.mcap;
     float *A = glob ? g.gA + roff * PP : A_s;
@@ -788,23 +827,23 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     float *U = g.U + roff * MAXR;
 
     const double h = tv.info->radius / (double)(1LL << lvl);
-    for (int p = tid; p < P; p += ID_THREADS) proxy_point<D>(p, h, prox + p * D);
+    for (int p = tid; p < P; p += IDG_THREADS) proxy_point<D>(p, h, prox + p * D);
     float ctr[D];
     for (int k = 0; k < D; k++)
         ctr[k] = (float)(tv.info->corner[k] + (double)(2 * tv.ix[(size_t)t * 3 + k] + 1) * h);
     if (LEAVES) {
-        for (int a = tid; a < m; a += ID_THREADS) cand[a] = xt[tv.start[t] + a];
+        for (int a = tid; a < m; a += IDG_THREADS) cand[a] = xt[tv.start[t] + a];
     } else {
-        for (int a = tid; a < m; a += ID_THREADS) {
-            int c = tv.fchild[t], aa = a;
-            while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
-            cand[a] = skel[(size_t)c * MAXR + aa];
+        for (int a = tid; a < m; a += IDG_THREADS) {
+            int c = 0;
+            while (a >= s_coff[c + 1]) c++;
+            cand[a] = __ldcg(skel + (size_t)(tv.fchild[t] + c) * MAXR + (a - s_coff[c]));
         }
     }
     __syncthreads();
 
     float lmax = 0.f;
-    for (int a = tid; a < m; a += ID_THREADS) {
+    for (int a = tid; a < m; a += IDG_THREADS) {
         const Vec<D> x = cand[a];
         float rel[D];
         for (int k = 0; k < D; k++) rel[k] = vget(x, k) - ctr[k];
@@ -826,7 +865,7 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     __syncthreads();
     if (tid == 0) {
         float v = 0.f;
-        for (int w = 0; w < ID_THREADS / 32; w++) v = fmaxf(v, s_bv[w]);
+        for (int w = 0; w < IDG_THREADS / 32; w++) v = fmaxf(v, s_bv[w]);
         s_n0 = v;
     }
     __syncthreads();
@@ -836,7 +875,7 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
     while (r < rmax) {
         float bv = -1.f;
         int bi = INT_MAX;
-        for (int a = tid; a < m; a += ID_THREADS)
+        for (int a = tid; a < m; a += IDG_THREADS)
             if (selpos[a] < 0 && (nrm[a] > bv)) { bv = nrm[a]; bi = a; }
         for (int o = 16; o > 0; o >>= 1) {
             const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -848,7 +887,7 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
         if (tid == 0) {
             float v = s_bv[0];
             int i = s_bi[0];
-            for (int w = 1; w < ID_THREADS / 32; w++)
+            for (int w = 1; w < IDG_THREADS / 32; w++)
                 if (s_bv[w] > v || (s_bv[w] == v && s_bi[w] < i)) { v = s_bv[w]; i = s_bi[w]; }
             s_best = i;
             s_stop = (i == INT_MAX) || !(v > stop2) || !(v > 0.f);
@@ -859,30 +898,45 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
         const float rr = sqrtf(nrm[best]);
         const float inv = 1.0f / rr;
         float *q = A + (size_t)best * PP;
-        for (int p = tid; p < P; p += ID_THREADS) q[p] *= inv;
+        for (int p = tid; p < P; p += IDG_THREADS) q[p] *= inv;
         if (tid == 0) { selpos[best] = r; sel[r] = best; }
         __syncthreads();
-        for (int a = tid; a < m; a += ID_THREADS) {
-            if (selpos[a] >= 0) continue;
-            float *row = A + (size_t)a * PP;
-            float dot = 0.f;
-            for (int p = 0; p < P; p++) dot = fmaf(q[p], row[p], dot);
-            float s2 = 0.f;
-            for (int p = 0; p < P; p++) { const float v = fmaf(-dot, q[p], row[p]); row[p] = v; s2 = fmaf(v, v, s2); }
-            nrm[a] = s2;
-            U[(size_t)a * MAXR + r] = dot;
+        // IDG_GROUP threads per row, each over every IDG_GROUP-th proxy; the partial sums meet by
+        // shuffles inside the group (whole warps take part in them)
+        for (int a0 = 0; a0 < m; a0 += IDG_THREADS / IDG_GROUP) {
+            const int a = a0 + tid / IDG_GROUP, gl = tid % IDG_GROUP;
+            const bool act = a < m && selpos[a] < 0;
+            float *row = A + (size_t)(act ? a : 0) * PP;
+            float d2[2] = {0.f, 0.f};
+            if (act)
+                for (int p = gl, j = 0; p < P; p += IDG_GROUP, j ^= 1) d2[j] = fmaf(q[p], row[p], d2[j]);
+            float dot = d2[0] + d2[1];
+            for (int o = 1; o < IDG_GROUP; o <<= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            float z2[2] = {0.f, 0.f};
+            if (act)
+                for (int p = gl, j = 0; p < P; p += IDG_GROUP, j ^= 1) {
+                    const float v = fmaf(-dot, q[p], row[p]);
+                    row[p] = v;
+                    z2[j] = fmaf(v, v, z2[j]);
+                }
+            float s2 = z2[0] + z2[1];
+            for (int o = 1; o < IDG_GROUP; o <<= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            if (act && gl == 0) {
+                nrm[a] = s2;
+                U[(size_t)a * MAXR + r] = dot;
+            }
         }
         __syncthreads();
         // column r of R11 (R[0..r-1][best] from the earlier steps, then the norm) into the
         // pivot row, which is dead from now on
-        for (int k = tid; k <= r; k += ID_THREADS) q[k] = k < r ? U[(size_t)best * MAXR + k] : rr;
+        for (int k = tid; k <= r; k += IDG_THREADS) q[k] = k < r ? U[(size_t)best * MAXR + k] : rr;
         r++;
     }
     __syncthreads();
-    for (int k = tid; k < r; k += ID_THREADS) skel[(size_t)t * MAXR + k] = cand[sel[k]];
+    for (int k = tid; k < r; k += IDG_THREADS) skel[(size_t)t * MAXR + k] = cand[sel[k]];
     if (tid == 0) g.rank[t] = r;
     // R11[k][j] = A[sel[j]][k]
-    for (int a = tid; a < m; a += ID_THREADS) {
+    for (int a = tid; a < m; a += IDG_THREADS) {
         float *u = U + (size_t)a * MAXR;
         const int pos = selpos[a];
         if (pos >= 0) {
@@ -895,39 +949,43 @@ __global__ void __launch_bounds__(ID_THREADS) k_id(int level, IdArgs g)
             }
         }
     }
-    // upward pass of this node: y0[t] = U^T (the leaf's [1 | x] | the children's y0)
+    // upward pass of this node: y0[t] = U^T (the leaf's [1 | x] | the children's y0), groups of
+    // RG threads over k and IDG_THREADS / RG groups over the rows, summed in a fixed order
     __syncthreads();
-    for (int k = tid; k < r; k += ID_THREADS) {
+    {
+        const int RG = r <= 16 ? 16 : (r <= 32 ? 32 : 64);
+        const int C = IDG_THREADS / RG, kk = tid % RG, cg = tid / RG;
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (LEAVES) {
-            for (int a = 0; a < m; a++) {
-                const float w = U[(size_t)a * MAXR + k];
-                const Vec<D> x = cand[a];
-                acc.x += w;
-                acc.y = fmaf(w, vget(x, 0), acc.y);
-                acc.z = fmaf(w, vget(x, 1), acc.z);
-                if (D == 3) acc.w = fmaf(w, vget(x, 2), acc.w);
-            }
-        } else {
-            int a = 0;
-            for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++)
-                for (int kk = 0; kk < g.rank[c]; kk++, a++) {
-                    const float w = U[(size_t)a * MAXR + k];
-                    const float4 y = g.y0[(size_t)c * MAXR + kk];
-                    acc.x = fmaf(w, y.x, acc.x); acc.y = fmaf(w, y.y, acc.y);
-                    acc.z = fmaf(w, y.z, acc.z); acc.w = fmaf(w, y.w, acc.w);
+        if (kk < r) {
+            for (int a = cg; a < m; a += C) {
+                const float w = U[(size_t)a * MAXR + kk];
+                if (LEAVES) {
+                    const Vec<D> x = cand[a];
+                    acc.x += w;
+                    acc.y = fmaf(w, vget(x, 0), acc.y);
+                    acc.z = fmaf(w, vget(x, 1), acc.z);
+                    if (D == 3) acc.w = fmaf(w, vget(x, 2), acc.w);
+                } else {
+                    int c = 0;
+                    while (a >= s_coff[c + 1]) c++;
+                    fma4(acc, w, __ldcg(g.y0 + (size_t)(tv.fchild[t] + c) * MAXR + (a - s_coff[c])));
                 }
+            }
         }
-        g.y0[(size_t)t * MAXR + k] = acc;
+        s_part[tid] = acc;
+        __syncthreads();
+        if (tid < r) {
+            float4 y = s_part[tid];
+            for (int c = 1; c < C; c++) add4(y, s_part[c * RG + tid]);
+            g.y0[(size_t)t * MAXR + tid] = y;
+        }
+    }
+    if (items != nullptr && !LEAVES) {
+        __syncthreads();
+        if (tid == 0) dep_publish(dp, t);
     }
 }
 
-__device__ __forceinline__ void fma4(float4 &acc, float w, const float4 &v)
-{
-    acc.x = fmaf(w, v.x, acc.x); acc.y = fmaf(w, v.y, acc.y);
-    acc.z = fmaf(w, v.z, acc.z); acc.w = fmaf(w, v.w, acc.w);
-}
-__device__ __forceinline__ void add4(float4 &a, const float4 &b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
 
 
 // Warp argmax of (norm, row): the largest norm, ties to the lowest row. Norms are >= 0 or -1
@@ -1723,6 +1781,10 @@ public:
             ListOut lo = list_out(1);
             k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
             launches_++;
+            if (D == 3) {
+                sort_segments(far_idx_, far_alt_, htot_[0], far_ptr_.p);
+                sort_segments(near_idx_, near_alt_, htot_[1], near_ptr_.p);
+            }
         }
         mark_end(t_lists, 1);
 
@@ -1772,17 +1834,18 @@ public:
             rank_stats_valid_ = false;
             return 0;
         }
-        k_id<D, true><<<n_node_ - first, ID_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il);
+        DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
+        k_id<D, true><<<n_node_ - first, IDG_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il, 0, nullptr, dp);
         launches_++;
         mark_end(t_bases, 2);
         t_bases = mark_begin();
-        // internal nodes, bottom-up (their candidates are the children's skeletons)
+        // internal nodes of every level in one dependency-ordered launch (their candidates are
+        // the children's skeletons)
         IdArgs ia = il;
         ia.mcap = mcap;
-        for (int l = max_level_ - 1; l >= MIN_ADM_LEVEL; l--) {
-            const int nl = I.n_level_nodes[l];
-            if (nl == 0) continue;
-            k_id<D, false><<<nl, ID_THREADS, id_smem_bytes<D>(mcap), st_>>>(l, ia);
+        if (hint_ > 0) {
+            TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
+            k_id<D, false><<<hint_, IDG_THREADS, id_smem_bytes<D>(mcap), st_>>>(0, ia, hint_, ilist_.p, dp);
             launches_++;
         }
         mark_end(t_bases, 7);
@@ -1999,7 +2062,7 @@ private:
     {
         // shared-memory rows of the ID: every internal node of the 2D tree (4 * MAXR rows)
         // and leaves up to that size; the 3D bound keeps the CTA under 227 KB
-        return D == 2 ? (1 << D) * Dim<D>::MAXR : 192;
+        return D == 2 ? (1 << D) * Dim<D>::MAXR : 240;
     }
 
     void alloc_nodes()
@@ -2045,6 +2108,20 @@ private:
         if (need > cub_tmp_.cap) cub_tmp_.exact(need + 256);
         size_t bytes = cub_tmp_.cap;
         TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(cub_tmp_.p, bytes, in, out + 1, count, st_));
+    }
+    // ascending order inside every node's segment [ptr[t], ptr[t + 1]) of idx (count entries)
+    void sort_segments(DevBuf<int> &idx, DevBuf<int> &alt, int count, const int *ptr)
+    {
+        if (count <= 1) return;
+        alt.ensure(count);
+        cub::DoubleBuffer<int> keys(idx.p, alt.p);
+        size_t need = 0;
+        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortKeys(nullptr, need, keys, count, n_node_, ptr, ptr + 1, st_));
+        if (need > cub_tmp_.cap) cub_tmp_.exact(need + 256);
+        size_t bytes = cub_tmp_.cap;
+        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortKeys(cub_tmp_.p, bytes, keys, count, n_node_, ptr, ptr + 1, st_));
+        if (keys.Current() != idx.p) idx.swap(alt);
+        launches_ += 2;
     }
     void scan_exclusive_ll(const int *in, long long *out, int count)
     {
@@ -2119,6 +2196,7 @@ private:
     DevBuf<int> flag_, ticket_;   // dependency-ordered launches
     int epoch_ = 0;
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;
+    DevBuf<int> far_alt_, near_alt_;   // segmented-sort partners of the 3D lists
     DevBuf<int> rowcap_;
     DevBuf<int> iflag_, ipos_, ilist_;   // internal nodes at level >= 2, in increasing id
     DevBuf<int> lflag_, lpos_, llist_;   // leaves at level >= 2 of at most LEAF_SMALL points

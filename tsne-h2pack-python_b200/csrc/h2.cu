@@ -1549,49 +1549,53 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
 }
 
 // downward pass of node t (one warp): the node's y1 through U onto its leaf points (yp) or
-// its children's y1. FRESH: y1 is read through L2 (written in the same launch).
+// its children's y1. y1 is staged in the warp's slice of shared memory (sy, MAXR entries); lane
+// a takes candidate row a and reads its U row four entries at a time. FRESH: y1 is read
+// through L2 (written in the same launch).
 template <int D, bool FRESH>
-__device__ __forceinline__ void down_node(const ProdArgs &g, int t, int lane)
+__device__ __forceinline__ void down_node(const ProdArgs &g, int t, int lane, float4 *sy)
 {
     constexpr int MAXR = Dim<D>::MAXR;
     const TreeView &tv = g.tv;
     const int r = g.rank[t];
     const float *U = g.U + g.rowoff[t] * MAXR;
-    float4 yr[MAXR / 32];
-    for (int h = 0; h < MAXR / 32; h++) {
-        const int k = lane + 32 * h;
+    for (int k = lane; k < r; k += 32) {
         const float4 *src = g.y1 + (size_t)t * MAXR + k;
-        yr[h] = k < r ? (FRESH ? __ldcg(src) : *src) : make_float4(0.f, 0.f, 0.f, 0.f);
+        sy[k] = FRESH ? __ldcg(src) : *src;
     }
+    __syncwarp();
     const bool isleaf = tv.leaf[t] != 0;
     int m = 0;
     if (isleaf) m = tv.end[t] - tv.start[t];
     else for (int c = tv.fchild[t]; c < tv.fchild[t] + tv.nchild[t]; c++) m += g.rank[c];
+    const int r4 = r & ~3;
     for (int a0 = 0; a0 < m; a0 += 32) {
         const int a = a0 + lane;
+        if (a >= m) break;
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int k = 0; k < r; k++) {
-            const float4 y = make_float4(__shfl_sync(0xffffffffu, yr[k >> 5].x, k & 31),
-                                         __shfl_sync(0xffffffffu, yr[k >> 5].y, k & 31),
-                                         __shfl_sync(0xffffffffu, yr[k >> 5].z, k & 31),
-                                         __shfl_sync(0xffffffffu, yr[k >> 5].w, k & 31));
-            if (a < m) fma4(acc, U[(size_t)a * MAXR + k], y);
+        const float *u = U + (size_t)a * MAXR;
+        for (int k = 0; k < r4; k += 4) {
+            const float4 w = *reinterpret_cast<const float4 *>(u + k);
+            fma4(acc, w.x, sy[k]);
+            fma4(acc, w.y, sy[k + 1]);
+            fma4(acc, w.z, sy[k + 2]);
+            fma4(acc, w.w, sy[k + 3]);
         }
-        if (a < m) {
-            if (isleaf) {
-                float4 o = g.yp[tv.start[t] + a];
-                add4(o, acc);
-                g.yp[tv.start[t] + a] = o;
-            } else {
-                int c = tv.fchild[t], aa = a;
-                while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
-                float4 *dst = g.y1 + (size_t)c * MAXR + aa;
-                float4 o = FRESH ? __ldcg(dst) : *dst;
-                add4(o, acc);
-                *dst = o;
-            }
+        for (int k = r4; k < r; k++) fma4(acc, u[k], sy[k]);
+        if (isleaf) {
+            float4 o = g.yp[tv.start[t] + a];
+            add4(o, acc);
+            g.yp[tv.start[t] + a] = o;
+        } else {
+            int c = tv.fchild[t], aa = a;
+            while (aa >= g.rank[c]) { aa -= g.rank[c]; c++; }
+            float4 *dst = g.y1 + (size_t)c * MAXR + aa;
+            float4 o = FRESH ? __ldcg(dst) : *dst;
+            add4(o, acc);
+            *dst = o;
         }
     }
+    __syncwarp();
 }
 
 // downward pass of every internal node at level >= 2 in one dependency-ordered launch
@@ -1600,6 +1604,7 @@ template <int D>
 __global__ void __launch_bounds__(256) k_down_internal(int n_item, const int *__restrict__ items, ProdArgs g,
                                                         DepArgs dp)
 {
+    __shared__ float4 sy[256 / 32][Dim<D>::MAXR];
     const int lane = threadIdx.x & 31;
     for (;;) {
         int item = 0;
@@ -1610,7 +1615,7 @@ __global__ void __launch_bounds__(256) k_down_internal(int n_item, const int *__
         const int p = g.tv.parent[t];
         if (lane == 0 && g.tv.level[p] >= MIN_ADM_LEVEL) dep_wait(dp, p);
         __syncwarp();
-        down_node<D, true>(g, t, lane);
+        down_node<D, true>(g, t, lane, sy[threadIdx.x >> 5]);
         __syncwarp();
         if (lane == 0) dep_publish(dp, t);
     }
@@ -1620,13 +1625,14 @@ __global__ void __launch_bounds__(256) k_down_internal(int n_item, const int *__
 template <int D>
 __global__ void __launch_bounds__(256) k_down_leaves(ProdArgs g)
 {
+    __shared__ float4 sy[256 / 32][Dim<D>::MAXR];
     const TreeView &tv = g.tv;
     const int lb = tv.info->level_begin[MIN_ADM_LEVEL];
     const int nl = tv.info->n_node - lb;
     const int lane = threadIdx.x & 31;
     for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nl; j += (gridDim.x * blockDim.x) >> 5) {
         const int t = lb + j;
-        if (tv.leaf[t]) down_node<D, false>(g, t, lane);
+        if (tv.leaf[t]) down_node<D, false>(g, t, lane, sy[threadIdx.x >> 5]);
     }
 }
 

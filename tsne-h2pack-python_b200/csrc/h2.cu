@@ -907,18 +907,27 @@ __global__ void __launch_bounds__(IDG_THREADS) k_id(int level, IdArgs g, int n_i
             const int a = a0 + tid / IDG_GROUP, gl = tid % IDG_GROUP;
             const bool act = a < m && selpos[a] < 0;
             float *row = A + (size_t)(act ? a : 0) * PP;
+            static_assert(P % IDG_GROUP == 0, "proxies split evenly over a row's threads");
             float d2[2] = {0.f, 0.f};
-            if (act)
-                for (int p = gl, j = 0; p < P; p += IDG_GROUP, j ^= 1) d2[j] = fmaf(q[p], row[p], d2[j]);
+            if (act) {
+#pragma unroll 6
+                for (int i = 0; i < P / IDG_GROUP; i++) {
+                    const int p = gl + i * IDG_GROUP;
+                    d2[i & 1] = fmaf(q[p], row[p], d2[i & 1]);
+                }
+            }
             float dot = d2[0] + d2[1];
             for (int o = 1; o < IDG_GROUP; o <<= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
             float z2[2] = {0.f, 0.f};
-            if (act)
-                for (int p = gl, j = 0; p < P; p += IDG_GROUP, j ^= 1) {
+            if (act) {
+#pragma unroll 6
+                for (int i = 0; i < P / IDG_GROUP; i++) {
+                    const int p = gl + i * IDG_GROUP;
                     const float v = fmaf(-dot, q[p], row[p]);
                     row[p] = v;
-                    z2[j] = fmaf(v, v, z2[j]);
+                    z2[i & 1] = fmaf(v, v, z2[i & 1]);
                 }
+            }
             float s2 = z2[0] + z2[1];
             for (int o = 1; o < IDG_GROUP; o <<= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
             if (act && gl == 0) {
@@ -935,17 +944,34 @@ __global__ void __launch_bounds__(IDG_THREADS) k_id(int level, IdArgs g, int n_i
     __syncthreads();
     for (int k = tid; k < r; k += IDG_THREADS) skel[(size_t)t * MAXR + k] = cand[sel[k]];
     if (tid == 0) g.rank[t] = r;
-    // R11[k][j] = A[sel[j]][k]
+    // R11[k][j] = A[sel[j]][k]; a node whose matrix lives in global memory first copies R11 into
+    // the (unused) shared-memory matrix area, column j at j (j + 1) / 2
+    const float *R11 = A;
+    if (glob) {
+        float *R = A_s;
+        for (int idx = tid; idx < r * r; idx += IDG_THREADS) {
+            const int j = idx / r, k = idx % r;
+            if (k <= j) R[j * (j + 1) / 2 + k] = A[(size_t)sel[j] * PP + k];
+        }
+        __syncthreads();
+        R11 = R;
+    }
     for (int a = tid; a < m; a += IDG_THREADS) {
         float *u = U + (size_t)a * MAXR;
         const int pos = selpos[a];
         if (pos >= 0) {
             for (int k = 0; k < r; k++) u[k] = (k == pos) ? 1.f : 0.f;
+        } else if (glob) {
+            for (int k = r - 1; k >= 0; k--) {
+                float acc = u[k];
+                for (int j = k + 1; j < r; j++) acc = fmaf(-R11[j * (j + 1) / 2 + k], u[j], acc);
+                u[k] = acc / R11[k * (k + 1) / 2 + k];
+            }
         } else {
             for (int k = r - 1; k >= 0; k--) {
                 float acc = u[k];
-                for (int j = k + 1; j < r; j++) acc = fmaf(-A[(size_t)sel[j] * PP + k], u[j], acc);
-                u[k] = acc / A[(size_t)sel[k] * PP + k];
+                for (int j = k + 1; j < r; j++) acc = fmaf(-R11[(size_t)sel[j] * PP + k], u[j], acc);
+                u[k] = acc / R11[(size_t)sel[k] * PP + k];
             }
         }
     }

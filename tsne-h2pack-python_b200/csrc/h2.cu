@@ -760,6 +760,47 @@ constexpr size_t id_smem_bytes(int mcap)
 // a step produces is stored in the pivot row of A, which no later step reads.
 // LEAVES = true: every leaf at level >= 2 (leaves depend on nothing), blockIdx.x counts
 // from the first node of level 2; false: the internal nodes of one level.
+// One Gram-Schmidt step over the candidate rows of A (row stride PP): every unselected row a
+// loses its component along the unit pivot row q; its dot product goes to U[a][r] and its new
+// squared norm to nrm[a]. G threads per row, each over every G-th proxy.
+template <int G, int P, int PP>
+__device__ __forceinline__ void gs_rows(float *A, const float *q, int m, int tid, const int *selpos, float *nrm,
+                                        float *U, int MAXR, int r)
+{
+    static_assert(P % G == 0, "proxies split evenly over a row's threads");
+    for (int a0 = 0; a0 < m; a0 += IDG_THREADS / G) {
+        const int a = a0 + tid / G, gl = tid % G;
+        const bool act = a < m && selpos[a] < 0;
+        float *row = A + (size_t)(act ? a : 0) * PP;
+        float d2[2] = {0.f, 0.f};
+        if (act) {
+#pragma unroll 6
+            for (int i = 0; i < P / G; i++) {
+                const int p = gl + i * G;
+                d2[i & 1] = fmaf(q[p], row[p], d2[i & 1]);
+            }
+        }
+        float dot = d2[0] + d2[1];
+        for (int o = 1; o < G; o <<= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+        float z2[2] = {0.f, 0.f};
+        if (act) {
+#pragma unroll 6
+            for (int i = 0; i < P / G; i++) {
+                const int p = gl + i * G;
+                const float v = fmaf(-dot, q[p], row[p]);
+                row[p] = v;
+                z2[i & 1] = fmaf(v, v, z2[i & 1]);
+            }
+        }
+        float s2 = z2[0] + z2[1];
+        for (int o = 1; o < G; o <<= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        if (act && gl == 0) {
+            nrm[a] = s2;
+            U[(size_t)a * MAXR + r] = dot;
+        }
+    }
+}
+
 // items != nullptr: the internal nodes of every level in one dependency-ordered launch (items
 // in increasing node id, taken deepest first; a node waits for its internal children's flags);
 // otherwise the nodes of `level` (or every leaf). Children's ranks, skeletons and coefficients
@@ -898,43 +939,18 @@ __global__ void __launch_bounds__(IDG_THREADS) k_id(int level, IdArgs g, int n_i
         const float rr = sqrtf(nrm[best]);
         const float inv = 1.0f / rr;
         float *q = A + (size_t)best * PP;
-        for (int p = tid; p < P; p += IDG_THREADS) q[p] *= inv;
+        for (int p = tid; p < P; p += IDG_THREADS) {
+            const float v = q[p] * inv;
+            q[p] = v;
+            if (glob) A_s[p] = v;   // the shared-memory matrix area is free for a global-memory node
+        }
         if (tid == 0) { selpos[best] = r; sel[r] = best; }
         __syncthreads();
-        // IDG_GROUP threads per row, each over every IDG_GROUP-th proxy; the partial sums meet by
-        // shuffles inside the group (whole warps take part in them)
-        for (int a0 = 0; a0 < m; a0 += IDG_THREADS / IDG_GROUP) {
-            const int a = a0 + tid / IDG_GROUP, gl = tid % IDG_GROUP;
-            const bool act = a < m && selpos[a] < 0;
-            float *row = A + (size_t)(act ? a : 0) * PP;
-            static_assert(P % IDG_GROUP == 0, "proxies split evenly over a row's threads");
-            float d2[2] = {0.f, 0.f};
-            if (act) {
-#pragma unroll 6
-                for (int i = 0; i < P / IDG_GROUP; i++) {
-                    const int p = gl + i * IDG_GROUP;
-                    d2[i & 1] = fmaf(q[p], row[p], d2[i & 1]);
-                }
-            }
-            float dot = d2[0] + d2[1];
-            for (int o = 1; o < IDG_GROUP; o <<= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-            float z2[2] = {0.f, 0.f};
-            if (act) {
-#pragma unroll 6
-                for (int i = 0; i < P / IDG_GROUP; i++) {
-                    const int p = gl + i * IDG_GROUP;
-                    const float v = fmaf(-dot, q[p], row[p]);
-                    row[p] = v;
-                    z2[i & 1] = fmaf(v, v, z2[i & 1]);
-                }
-            }
-            float s2 = z2[0] + z2[1];
-            for (int o = 1; o < IDG_GROUP; o <<= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-            if (act && gl == 0) {
-                nrm[a] = s2;
-                U[(size_t)a * MAXR + r] = dot;
-            }
-        }
+        // G threads per row, each over every G-th proxy; the partial sums meet by shuffles inside
+        // the group (whole warps take part in them). A matrix in global memory uses G = 8 and the
+        // pivot row staged in shared memory, for more loads in flight per row.
+        if (glob) gs_rows<8, P, PP>(A, A_s, m, tid, selpos, nrm, U, MAXR, r);
+        else gs_rows<IDG_GROUP, P, PP>(A, q, m, tid, selpos, nrm, U, MAXR, r);
         __syncthreads();
         // column r of R11 (R[0..r-1][best] from the earlier steps, then the norm) into the
         // pivot row, which is dead from now on

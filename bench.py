@@ -252,7 +252,7 @@ def ours(args, rank, world, local):
             "config": {"workload": f"{n:,} points x 50 dims -> 2D, {args.iters} iterations, perplexity 30, "
                                    "h2_tol 1e-2, H2 rebuild every 3 (10 early), leaf 100, init random",
                        "n_points": n, "nnz_P": int(nnz), "iterations": args.iters,
-                       "l2": "inputs larger than L2 (P streams 1.2 GB per iteration)",
+                       "l2": f"inputs larger than L2 (P streams {8 * nnz / 1e9:.2f} GB per iteration)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,

@@ -228,6 +228,12 @@ TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, lon
 TSNE_API int tsne_exact_repulsion_static(const float *Y, int n_point, int low_dim, float *F, double *Z,
                                          void *stream);
 
+/* Device memory: workspaces take their buffers from the current device's stream-ordered
+ * memory pool, which keeps freed memory for the next workspace (no counterpart in the
+ * reference, which allocates on the host). This returns the pool's unused memory to the
+ * driver; 0 on success. */
+TSNE_API int tsne_release_cached_memory(void);
+
 /* ---- Batched and served jobs (no counterpart in the reference, which runs one embedding
  * per call). A server runs many independent optimisations on the current device: jobs queue
  * in arrival order and start when fewer than max_concurrent run and their device memory
@@ -254,7 +260,8 @@ TSNE_API tsne_server_t *tsne_server_create(int max_concurrent, double hbm_budget
 TSNE_API int tsne_server_submit(tsne_server_t *s, int n_point, int low_dim, const tsne_params_t *params,
                                 sparse_matrix_t *P);
 /* Blocks until the job ends; Y_out (low_dim x n_point, may be NULL) and info (may be NULL)
- * receive the result. Returns 0, or -1 when the job failed or was cancelled. */
+ * receive the result, which the server then releases (a second wait returns the info and -1).
+ * Returns 0, or -1 when the job failed, was cancelled or was already collected. */
 TSNE_API int tsne_server_wait(tsne_server_t *s, int job, DTYPE *Y_out, tsne_job_info_t *info);
 /* Jobs queued or running. */
 TSNE_API int tsne_server_pending(tsne_server_t *s);

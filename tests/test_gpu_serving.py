@@ -50,6 +50,13 @@ def test_batch_results_equal_alone(jobs):
     with EmbeddingServer(max_concurrent=4, hbm_budget_gb=100.0) as srv:
         ids = [_submit(srv, P, Y0, n_iter) for P, Y0 in jobs]
         res = [srv.wait(j) for j in ids]
+        # a collected result is released: a second wait reports the job but returns -1
+        import ctypes
+        from tsne_h2pack.serving import JobInfo
+        info = JobInfo()
+        assert srv._lib.tsne_server_wait(srv._h, ids[0], None, ctypes.byref(info)) == -1
+        assert info.status == 0 and info.n_point == jobs[0][0].shape[0]
+    assert srv._lib.tsne_release_cached_memory() == 0
     for (Yr, klr), (Y, info) in zip(ref, res):
         assert info.ok
         np.testing.assert_array_equal(Y.T, Yr)

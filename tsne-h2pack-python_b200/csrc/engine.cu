@@ -86,6 +86,16 @@ __global__ void k_conv_check(int n, const float *__restrict__ Y, const float *__
 
 }  // namespace
 
+extern "C" TSNE_API int tsne_release_cached_memory(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return -1;
+    if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+    return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? 0 : -1;
+}
+
 namespace tsne {
 void keep_pool_memory()
 {

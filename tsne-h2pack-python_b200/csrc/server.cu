@@ -44,6 +44,7 @@ struct Job {
     sparse_matrix_t *P = nullptr;   // owned until the workspace takes it
     size_t bytes = 0;               // admission estimate
     int state = QUEUED;
+    bool collected = false;         // the result was handed out and released
     std::vector<double> Y;          // result, low_dim x n
     double kl = 0.0;
     double t_submit = 0.0, t_start = 0.0, t_end = 0.0, run_s = 0.0;
@@ -199,8 +200,11 @@ int tsne_server_wait(tsne_server_t *s, int job_id, double *Y_out, tsne_job_info_
         info->start_s = job->t_start;
         info->end_s = job->t_end;
     }
-    if (job->state != DONE) return -1;
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (job->state != DONE || job->collected) return -1;
     if (Y_out != nullptr) memcpy(Y_out, job->Y.data(), sizeof(double) * job->Y.size());
+    job->collected = true;
+    std::vector<double>().swap(job->Y);   // a long-running server keeps no finished embeddings
     return 0;
 }
 

@@ -55,6 +55,8 @@ def _bind(lib):
     lib.tsne_server_pending.restype = ctypes.c_int
     lib.tsne_server_destroy.argtypes = [ctypes.c_void_p]
     lib.tsne_server_destroy.restype = None
+    lib.tsne_release_cached_memory.argtypes = []
+    lib.tsne_release_cached_memory.restype = ctypes.c_int
     lib._server_bound = True
 
 

@@ -1390,6 +1390,36 @@ __global__ void __launch_bounds__(256) k_far_c(int first, int n_node, ProdArgs g
     for (int t = first + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t < n_node;
          t += (gridDim.x * blockDim.x) >> 5) {
         const int r = g.rank[t], lt = tv.level[t];
+        if (r <= 32) {
+            // rank <= 32: groups of rp lanes (rp = r rounded up to a power of two) take one
+            // target slot each and the warp's 32 / rp groups split the sources; the group sums
+            // meet by shuffles in a fixed order
+            int rp = 1;
+            while (rp < r) rp <<= 1;
+            const int S = 32 / rp, k = lane % rp, sub = lane / rp;
+            const Vec<D> Jk = skel[(size_t)t * MAXR + (k < r ? k : 0)];
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++) {
+                const int s = g.far_idx[e];
+                const int ls = tv.level[s];
+                if (ls == lt) {
+                    const int rs = g.rank[s];
+                    for (int b = sub; b < rs; b += S)
+                        fma4(acc, rkernel(dist2(Jk, skel[(size_t)s * MAXR + b])), g.y0[(size_t)s * MAXR + b]);
+                } else if (ls < lt) {
+                    for (int j = tv.start[s] + sub; j < tv.end[s]; j += S)
+                        fma4(acc, rkernel(dist2(Jk, xt[j])), input_at<D>(g, xt, j));
+                }
+            }
+            for (int o = rp; o < 32; o <<= 1) {
+                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+                acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+                acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+            }
+            if (sub == 0 && k < r) g.y1[(size_t)t * MAXR + k] = acc;
+            continue;
+        }
         Vec<D> J[MAXR / 32];
         float4 acc[MAXR / 32];
         for (int h = 0; h < MAXR / 32; h++) {

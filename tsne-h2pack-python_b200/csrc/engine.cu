@@ -573,6 +573,10 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
     TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     if (it_end >= n_iter || ret != 0) ws->kl = ws->hsc.p->kl;
+    if (ret == 0 && ws->h2 && ws->h2->wait_failed()) {
+        fprintf(stderr, "ERROR: an H2 kernel gave up waiting for a tree dependency; the run is not valid\n");
+        ret = -1;
+    }
     {
         float ms = 0.f;
         TSNE_CUDA_CHECK(cudaEventElapsedTime(&ms, run0, run1));

@@ -2078,6 +2078,14 @@ public:
 
     long long launches() const override { return launches_; }
 
+    int wait_failed() override
+    {
+        TreeInfo I;
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        TSNE_CUDA_CHECK(cudaMemcpy(&I, info_.p, sizeof(TreeInfo), cudaMemcpyDeviceToHost));
+        return I.pad[1] != 0;
+    }
+
     // TSNE_H2_TIMERS=1: device time per phase (CUDA events on the stream), summed over builds
     // and products until flush_timers() prints them
     void flush_timers() override

@@ -42,6 +42,9 @@ public:
     virtual void copy_lists(int *far_ptr, int *far_idx, int *near_ptr, int *near_idx) = 0;
     virtual void copy_ranks(int *rank) = 0;
     virtual long long launches() const = 0;
+    // 1 when a bounded wait of a dependency-ordered launch gave up since the last build
+    // (its results are not to be trusted); synchronises the stream
+    virtual int wait_failed() = 0;
     // prints and clears the per-phase device times gathered under TSNE_H2_TIMERS=1
     virtual void flush_timers() = 0;
 };

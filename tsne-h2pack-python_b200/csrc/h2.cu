@@ -38,7 +38,6 @@ namespace {
 
 template <int D> using Vec = typename Dim<D>::vec;
 
-constexpr int ID_THREADS = 128;
 constexpr int IDG_THREADS = 256;     // shared-memory ID kernel (3D, large 2D leaves)
 constexpr int IDG_GROUP = 4;         // its threads per candidate row in a Gram-Schmidt step
 constexpr int NEAR_THREADS = 128;

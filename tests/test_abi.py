@@ -133,3 +133,29 @@ def test_server_rejects_bad_arguments_without_a_device():
     assert not lib.tsne_server_create(2, 0.0)
     assert lib.tsne_server_submit(None, 10, 2, None, None) == -1
     assert lib.tsne_server_pending(None) == -1
+
+
+@pytest.mark.parametrize("case", ["first_not_zero", "decreasing"])
+def test_init_rejects_bad_row_pointers_before_the_device(case, capfd):
+    """tsne_init_with_P checks P's row pointers on the host before it creates any device state
+    (NULL, P left with the caller, as on a wrong shape)."""
+    import numpy as np
+    from scipy.sparse import csr_matrix
+    from tsne_h2pack._backend import get_backend, scipy_csr_to_c_sparse_matrix
+    be = get_backend()
+    lib = be._lib
+    n = 50
+    P = csr_matrix(np.eye(n, k=1) + np.eye(n, k=-1))
+    Pc = scipy_csr_to_c_sparse_matrix(P, lib)
+    rp = Pc.contents.row_ptr
+    if case == "first_not_zero":
+        rp[0] = 1
+    else:
+        rp[10], rp[11] = rp[11], rp[10]
+    params = be.create_default_params()
+    params.verbose = 0
+    ws = lib.tsne_init_with_P(None, n, 0, 2, ctypes.byref(params), Pc)
+    ctypes.CDLL(None).fflush(None)
+    assert not ws
+    assert "row pointers" in capfd.readouterr().out
+    lib.sparse_matrix_destroy(Pc)

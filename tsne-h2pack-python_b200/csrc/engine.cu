@@ -175,20 +175,48 @@ PinnedStage &pinned_stage()
     return s;
 }
 
-void fill_chunk(const int *ci, const double *pv, size_t count, int *col, float *val)
+// A column index outside [0, n) in the caller's P: the device would gather out of bounds, so
+// the upload stops and tsne_init_with_P returns NULL, leaving P with the caller (as on a
+// wrong shape).
+struct BadColumn {};
+
+// Copies one chunk of P into the staging buffers (values rounded to float) and checks every
+// column index against [0, n) on the way; false if one is out of range.
+bool fill_chunk(const int *ci, const double *pv, size_t count, int n, int *col, float *val)
 {
     const size_t per = size_t(1) << 20;
     const int nth = (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)std::max(1u, std::thread::hardware_concurrency()),
                                                              (count + per - 1) / per}));
+    std::vector<unsigned char> bad(nth, 0);
     auto work = [&](int k) {
         const size_t b = count * k / nth, e = count * (k + 1) / nth;
-        memcpy(col + b, ci + b, sizeof(int) * (e - b));
+        unsigned int out = 0;
+        for (size_t i = b; i < e; i++) {
+            const int c = ci[i];
+            out |= (unsigned int)c >= (unsigned int)n;
+            col[i] = c;
+        }
         for (size_t i = b; i < e; i++) val[i] = (float)pv[i];
+        bad[k] = out != 0;
     };
     std::vector<std::thread> th;
     for (int k = 1; k < nth; k++) th.emplace_back(work, k);
     work(0);
     for (auto &t : th) t.join();
+    for (unsigned char b : bad)
+        if (b) return false;
+    return true;
+}
+
+// Row pointers of the caller's P: start at 0 and never decrease (so every row range lies in
+// [0, nnz)), arrays present when there are entries.
+bool csr_rows_valid(const sparse_matrix_t *P)
+{
+    const int n = P->n_rows;
+    if (P->row_ptr == nullptr || P->row_ptr[0] != 0) return false;
+    for (int i = 0; i < n; i++)
+        if (P->row_ptr[i + 1] < P->row_ptr[i]) return false;
+    return P->row_ptr[n] == 0 || (P->col_idx != nullptr && P->values != nullptr);
 }
 
 void upload_P(tsne_workspace *ws)
@@ -217,17 +245,22 @@ void upload_P(tsne_workspace *ws)
         cudaEvent_t ev[2];
         for (int b = 0; b < 2; b++) TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
         size_t i = 0;
+        bool cols_ok = true;
         for (size_t c0 = 0; c0 < (size_t)nnz; c0 += CHUNK, i++) {
             const int b = (int)(i & 1);
             if (i >= 2) TSNE_CUDA_CHECK(cudaEventSynchronize(ev[b]));
             const size_t cnt = std::min(CHUNK, (size_t)nnz - c0);
-            fill_chunk(ws->P->col_idx + c0, ws->P->values + c0, cnt, ps.col[b], ps.val[b]);
+            if (!fill_chunk(ws->P->col_idx + c0, ws->P->values + c0, cnt, n, ps.col[b], ps.val[b])) {
+                cols_ok = false;
+                break;
+            }
             TSNE_CUDA_CHECK(cudaMemcpyAsync(ci0.p + c0, ps.col[b], sizeof(int) * cnt, cudaMemcpyHostToDevice, st));
             TSNE_CUDA_CHECK(cudaMemcpyAsync(pv0.p + c0, ps.val[b], sizeof(float) * cnt, cudaMemcpyHostToDevice, st));
             TSNE_CUDA_CHECK(cudaEventRecord(ev[b], st));
         }
         TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
         for (int b = 0; b < 2; b++) cudaEventDestroy(ev[b]);
+        if (!cols_ok) throw BadColumn();
     }
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     if (tm) printf("E2E upload_P: alloc + copies %.1f ms\n", 1e3 * (wall_sec() - t0));
@@ -807,6 +840,10 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         return nullptr;
     }
     if (params == nullptr || n_point < 1) return nullptr;
+    if (!csr_rows_valid(P)) {
+        printf("Error: Invalid P matrix (row pointers must start at 0 and not decrease)\n");
+        return nullptr;
+    }
     tsne_workspace *ws = new tsne_workspace();
     try {
         ws->params = *params;
@@ -873,6 +910,11 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         TSNE_CUDA_CHECK(cudaStreamSynchronize(ws->st));
         if (tm) printf("E2E init: first H2 build %.1f ms\n", 1e3 * (wall_sec() - t0));
     } catch (const CudaError &) {
+        tsne_destroy(ws);
+        return nullptr;
+    } catch (const BadColumn &) {
+        printf("Error: Invalid P matrix (a column index is outside [0, %d))\n", n_point);
+        ws->P = nullptr;   // P stays with the caller
         tsne_destroy(ws);
         return nullptr;
     }
@@ -1009,6 +1051,7 @@ void compute_attractive_forces(const sparse_matrix_t *P, const double *Y, int lo
 {
     (void)num_threads;
     if (P == nullptr || Y == nullptr || grad == nullptr || (low_dim != 2 && low_dim != 3)) return;
+    if (P->n_rows != n_point || P->n_cols != n_point || !csr_rows_valid(P)) return;
     sparse_matrix_t *Pc = sparse_matrix_create(P->n_rows, P->n_cols, P->row_ptr[P->n_rows]);
     if (Pc == nullptr) return;
     memcpy(Pc->row_ptr, P->row_ptr, sizeof(int) * (P->n_rows + 1));
@@ -1030,6 +1073,7 @@ void compute_attractive_forces(const sparse_matrix_t *P, const double *Y, int lo
         TSNE_CUDA_CHECK(cudaMemcpyAsync(grad, g.p, sizeof(double) * n_point * low_dim, cudaMemcpyDeviceToHost, ws.st));
         TSNE_CUDA_CHECK(cudaStreamSynchronize(ws.st));
     } catch (const CudaError &) {
+    } catch (const BadColumn &) {   // grad is left unchanged
     }
     sparse_matrix_destroy(Pc);
     ws.P = nullptr;

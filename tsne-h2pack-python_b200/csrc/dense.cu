@@ -75,10 +75,10 @@ __device__ __forceinline__ void row_attr(int b, int e, int lane, const Vec<D> &y
 
 // Block-wide FP64 reduction of per-warp values held by lane 0 of each warp, summed in
 // warp order; the result is valid in thread 0.
-template <int NV>
+template <int NV, int NW = ROW_BLOCK / 32>
 __device__ __forceinline__ void block_sum_warps(double (&v)[NV], double *out)
 {
-    __shared__ double sh[ROW_BLOCK / 32][NV];
+    __shared__ double sh[NW][NV];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0)
         for (int k = 0; k < NV; k++) sh[w][k] = v[k];
@@ -86,7 +86,7 @@ __device__ __forceinline__ void block_sum_warps(double (&v)[NV], double *out)
     if (threadIdx.x == 0) {
         for (int k = 0; k < NV; k++) {
             double s = 0.0;
-            for (int ww = 0; ww < ROW_BLOCK / 32; ww++) s += sh[ww][k];
+            for (int ww = 0; ww < NW; ww++) s += sh[ww][k];
             out[k] = s;
         }
     }
@@ -224,15 +224,162 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
 }
 
+// The same step with the Y gathers served from shared memory (TSNE_ATTR_WINDOW=1; off by
+// default). One CTA per SM owns a contiguous range of rows holding an equal share of P's
+// entries and stages the window of Y centred on it (win_pts points, 128 KB) once; a column
+// inside the window is read from shared memory, one outside it through L1/L2. After the
+// renumbering in tree order about three quarters of a point's neighbours lie inside a
+// 16K-point window around it (200K-point 2D embedding of the benchmark mixture), so most
+// gathers skip the L1 tag stage that bounds k_attr_update. Measured at 1M points, 2D: 0.651 ms
+// per launch against k_attr_update's 0.636 ms, so not faster (it keeps 32 warps per SM
+// resident instead of 64, and about a quarter of the gathers still go to L1/L2), hence off by
+// default. Splitting rows by equal counts instead of equal entries made it 1.25 ms: row
+// lengths follow the tree order's clusters. Used while the average CTA's row range fits in
+// half a window (n <= 148 * win_pts / 2). The row of each half-warp and the summation order
+// are fixed, so results are bit-reproducible, and the three modes give the same bits as one
+// another.
+constexpr int WIN_THREADS = 1024;
+constexpr int WIN_GRID = 148;
+template <int D> constexpr int win_pts() { return D == 2 ? 16384 : 8192; }
+
+// first row i in [0, n] with rp[i] >= x (rp non-decreasing, rp[0] = 0)
+__device__ __forceinline__ int first_row_at(const int *__restrict__ rp, int n, long long x)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)rp[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int D, int MODE>
+__global__ void __launch_bounds__(WIN_THREADS, 1)
+k_attr_window(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+              float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
+{
+    constexpr int WIN = win_pts<D>();
+    constexpr int NH = WIN_THREADS / 16;   // half-warps per CTA
+    extern __shared__ __align__(16) unsigned char win_raw[];
+    Vec<D> *win = reinterpret_cast<Vec<D> *>(win_raw);
+    const int lane = threadIdx.x & 31, hl = lane & 15, hw = threadIdx.x >> 4;
+    // CTA b takes the rows whose entries start in [b nnz / G, (b + 1) nnz / G): equal shares of
+    // P, since row lengths follow the clusters of the tree order and equal row counts would not
+    // balance; the last CTA also takes the empty rows at the end
+    const long long nnz = rp[n];
+    const int rb = first_row_at(rp, n, (long long)blockIdx.x * nnz / gridDim.x);
+    const int re = blockIdx.x + 1 == gridDim.x ? n : first_row_at(rp, n, (long long)(blockIdx.x + 1) * nnz / gridDim.x);
+    int w0 = rb + (re - rb) / 2 - WIN / 2;
+    w0 = max(0, min(w0, n - WIN));
+    const int wl = min(WIN, n - w0);
+    if (MODE != ATTR_UPDATE) {
+        for (int k = threadIdx.x; k < wl; k += WIN_THREADS) win[k] = Y[w0 + k];
+        __syncthreads();
+    }
+    const int use_rep = (MODE != ATTR_GRAD && rep != nullptr) ? *rep_flag : 0;
+    double acc[D];
+    for (int k = 0; k < D; k++) acc[k] = 0.0;
+    // every half-warp of the CTA runs the same number of rounds (full-warp shuffles)
+    const int rounds = (re - rb + NH - 1) / NH;
+    for (int rd = 0; rd < rounds; rd++) {
+        const int i = rb + rd * NH + hw;
+        const bool live = i < re;
+        Vec<D> yi = vzero<D>(), opnd = vzero<D>();
+        int b = 0, e = 0;
+        if (live) {
+            yi = Y[i];
+            b = rp[i];
+            e = rp[i + 1];
+            if (MODE != ATTR_GRAD) {
+                if (hl == 1) opnd = uY[i];
+                else if (hl == 2) opnd = gains[i];
+                else if (hl == 3 && use_rep) opnd = rep[i];
+            }
+        }
+        float a[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) a[k] = 0.f;
+        if (MODE == ATTR_UPDATE) {
+            if (live && hl == 0) {
+                const Vec<D> s = attr[i];
+#pragma unroll
+                for (int k = 0; k < D; k++) a[k] = vget(s, k);
+            }
+        } else {
+            for (int base = b + 4 * hl; base < e; base += 64) {
+                const int4 c4 = ld_stream_i4(col + base);
+                const float4 p4 = ld_stream_f4(val + base);
+                const int cs[4] = {c4.x, c4.y, c4.z, c4.w};
+                const float ps[4] = {p4.x, p4.y, p4.z, p4.w};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const unsigned int off = (unsigned int)(cs[q] - w0);
+                    const Vec<D> yj = off < (unsigned int)wl ? win[off] : __ldg(Y + cs[q]);
+                    float df[D], r2 = 0.f;
+#pragma unroll
+                    for (int k = 0; k < D; k++) { df[k] = vget(yi, k) - vget(yj, k); r2 = fmaf(df[k], df[k], r2); }
+                    const float w = ps[q] * fast_rcp(1.0f + r2);
+#pragma unroll
+                    for (int k = 0; k < D; k++) a[k] = fmaf(w, df[k], a[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+        }
+        if (MODE == ATTR_GRAD) {
+            if (live && hl == 0) {
+                Vec<D> s = vzero<D>();
+#pragma unroll
+                for (int k = 0; k < D; k++) vset(s, k, a[k]);
+                attr[i] = s;
+            }
+            continue;
+        }
+        const int src = lane & 16;
+        Vec<D> u = vzero<D>(), g = vzero<D>(), r = vzero<D>();
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            vset(u, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 1));
+            vset(g, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 2));
+            vset(r, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 3));
+        }
+        if (live && hl == 0) {
+            Vec<D> yn = yi;
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                const float gk = exag4 * a[k] - vget(r, k);
+                const float uk = vget(u, k);
+                float gain = (uk * gk < 0.f) ? vget(g, k) + 0.2f : vget(g, k) * 0.8f;
+                gain = fmaxf(gain, 0.01f);
+                const float un = mom * uk - lr * (gk * gain);
+                vset(g, k, gain);
+                vset(u, k, un);
+                vset(yn, k, vget(yi, k) + un);
+                acc[k] += (double)vget(yn, k);
+            }
+            uY[i] = u;
+            gains[i] = g;
+            Yn[i] = yn;
+        }
+    }
+    if (MODE == ATTR_GRAD) return;
+    for (int k = 0; k < D; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
+    block_sum_warps<D, WIN_THREADS / 32>(acc, partials + (size_t)blockIdx.x * D);
+}
+
 // Centring (reference tsne_h2pack.c:1978-1984): Y = Ynext - mean(Ynext), the mean summed
 // in FP64 from the update's fixed per-block partials, identically in every block.
 template <int D>
 __global__ void __launch_bounds__(RED_BLOCK)
 k_center(int n, const Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ Y, const double *__restrict__ partials,
-         DevScalars *sc)
+         int nblk, DevScalars *sc)
 {
     __shared__ double mean[D];
-    reduce_partials<D>(partials, ROW_GRID, mean);
+    reduce_partials<D>(partials, nblk, mean);
     if (threadIdx.x == 0) {
         for (int k = 0; k < D; k++) mean[k] /= (double)n;
         if (blockIdx.x == 0)
@@ -542,11 +689,42 @@ inline int ew_grid(int n) { int g = ceil_div(n, EW_BLOCK); return g < 1 ? 1 : (g
 // ---------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------
+// The shared-memory window form of the attractive step (k_attr_window) is taken while every
+// CTA's row range fits in half a window, when TSNE_ATTR_WINDOW=1; all three modes and the
+// centring follow the same rule, so a step's kernels always agree on the row split.
+template <int D>
+bool use_window(int n)
+{
+    static const bool on = [] {
+        const char *e = getenv("TSNE_ATTR_WINDOW");
+        return e != nullptr && atoi(e) != 0;
+    }();
+    return on && ceil_div(n, WIN_GRID) <= win_pts<D>() / 2;
+}
+template <int D, int MODE>
+void launch_window(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
+                   void *Ynext, void *uY, void *gains, const void *rep, const int *rep_flag, float exag4, float mom,
+                   float lr, double *partials, void *attr)
+{
+    constexpr size_t smem = MODE == ATTR_UPDATE ? 0 : sizeof(Vec<D>) * (size_t)win_pts<D>();
+    static const cudaError_t attr_set =
+        cudaFuncSetAttribute(k_attr_window<D, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    (void)attr_set;
+    k_attr_window<D, MODE><<<WIN_GRID, WIN_THREADS, smem, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains, (const Vec<D> *)rep,
+        rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+}
+
 template <int D>
 void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
                         const int *rep_flag, float exag4, float mom, float lr, double *partials)
 {
+    if (use_window<D>(n)) {
+        launch_window<D, ATTR_FUSED>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                     partials, nullptr);
+        return;
+    }
     k_attr_update<D, ATTR_FUSED><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
         (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
@@ -555,6 +733,11 @@ template <int D>
 void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
                       void *attr)
 {
+    if (use_window<D>(n)) {
+        launch_window<D, ATTR_GRAD>(st, n, rp, col, val, Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f,
+                                    0.f, nullptr, attr);
+        return;
+    }
     k_attr_update<D, ATTR_GRAD><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, col, val, (const Vec<D> *)Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, 0.f, nullptr,
         (Vec<D> *)attr);
@@ -564,6 +747,11 @@ void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Y
                    const void *rep, const int *rep_flag, const void *attr, float exag4, float mom, float lr,
                    double *partials)
 {
+    if (use_window<D>(n)) {
+        launch_window<D, ATTR_UPDATE>(st, n, rp, nullptr, nullptr, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom,
+                                      lr, partials, const_cast<void *>(attr));
+        return;
+    }
     k_attr_update<D, ATTR_UPDATE><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, nullptr, nullptr, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
         (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
@@ -573,7 +761,8 @@ template <int D>
 void launch_center(cudaStream_t st, int n, const void *Ynext, void *Ycur, const double *partials,
                    DevScalars *sc, const void *, double *)
 {
-    k_center<D><<<ew_grid(n), RED_BLOCK, 0, st>>>(n, (const Vec<D> *)Ynext, (Vec<D> *)Ycur, partials, sc);
+    const int nblk = use_window<D>(n) ? WIN_GRID : ROW_GRID;
+    k_center<D><<<ew_grid(n), RED_BLOCK, 0, st>>>(n, (const Vec<D> *)Ynext, (Vec<D> *)Ycur, partials, nblk, sc);
 }
 
 template <int D>

@@ -6,9 +6,10 @@ embeddings are (d, n) dimension-major float64, P is CSR with int32 indices.
 
 Two native libraries back it:
   _build/liboracle.so   this project's C restatement (tsne_oracle.c)
-  _ref/libtsne_ref.so   the reference's own sources compiled against ref_shim/ (exact
-                        repulsion path only; absent when the reference was not available
-                        at build time)
+  _ref/libtsne_ref.so   the reference's own sources compiled against ref_shim/: its exact
+                        repulsion path, and its H2 product and force code run on a matrix
+                        the oracle built (absent when the reference was not available at
+                        build time)
 """
 import ctypes
 import os
@@ -87,6 +88,11 @@ def lib():
         L.ora_h2_nodes.argtypes = [ctypes.c_void_p] + [_i32p] * 7
         L.ora_h2_lists.argtypes = [ctypes.c_void_p] + [_i32p] * 4
         L.ora_h2_ranks.argtypes = [ctypes.c_void_p, _i32p]
+        L.ora_h2_bases.argtypes = [ctypes.c_void_p, _i32p, _i32p, _i32p]
+        L.ora_h2_U.argtypes = [ctypes.c_void_p]
+        L.ora_h2_U.restype = _f64p
+        L.ora_h2_skel.argtypes = [ctypes.c_void_p]
+        L.ora_h2_skel.restype = _f64p
         L.ora_h2_n_proxy.argtypes = [ctypes.c_int]
         L.ora_h2_n_proxy.restype = ctypes.c_int
         L.ora_h2_proxies.argtypes = [ctypes.c_int, ctypes.c_double, _f64p]
@@ -219,6 +225,17 @@ class H2:
         lib().ora_h2_ranks(self._h, _p(r, _i32p))
         return r
 
+    def bases(self):
+        """(ncand, skel_off, U_off, U, skel): per node the candidate rows of its U block,
+        offsets of its skeleton points and of its U block (n_node + 1 entries each); U blocks
+        are ncand x rank row-major, skeleton points d coordinates each."""
+        m = self.n_node
+        ncand = np.zeros(m, np.int32); so = np.zeros(m + 1, np.int32); uo = np.zeros(m + 1, np.int32)
+        lib().ora_h2_bases(self._h, _p(ncand, _i32p), _p(so, _i32p), _p(uo, _i32p))
+        U = np.ctypeslib.as_array(lib().ora_h2_U(self._h), shape=(max(int(uo[-1]), 1),)).copy()
+        skel = np.ctypeslib.as_array(lib().ora_h2_skel(self._h), shape=(max(int(so[-1]) * self.d, 1),)).copy()
+        return ncand, so, uo, U, skel
+
     def product(self, Y=None, nthreads=None):
         Y = self.Y if Y is None else np.ascontiguousarray(Y, dtype=np.float64)
         s = np.zeros(self.n); v = np.zeros((self.d, self.n))
@@ -327,6 +344,13 @@ def ref_lib():
         L.compute_kl_divergence.restype = ctypes.c_double
         L.initialize_embedding.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p,
                                            ctypes.c_uint]
+        L.shim_h2_assemble.argtypes = ([ctypes.c_int] * 4 + [_i32p, _f64p] + [_i32p] * 6 +
+                                       [ctypes.c_int, _i32p, ctypes.c_int, _i32p, _i32p, _i32p, _f64p, _i32p,
+                                        _f64p, _i32p])
+        L.shim_h2_assemble.restype = ctypes.c_void_p
+        L.shim_h2_free.argtypes = [ctypes.c_void_p]
+        L.shim_ref_repulsion.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int, ctypes.c_int, _f64p]
+        L.shim_ref_repulsion.restype = ctypes.c_double
         _ref = L
     return _ref
 
@@ -418,3 +442,36 @@ class Runner:
 
     def __del__(self):
         self.close()
+
+
+def ref_h2_repulsion(h2, Y=None):
+    """The reference's compute_repulsive_forces_h2pack (src/tsne_h2pack.c:389-630, with its
+    fused product src/tsne_h2_matmul.c:225-452) run on the H2 matrix `h2` that the oracle
+    built: returns (F, Z), F (d, n) in the caller's order."""
+    L = ref_lib()
+    Y = h2.Y if Y is None else np.ascontiguousarray(Y, dtype=np.float64)
+    d, n = Y.shape
+    nodes = h2.nodes()
+    perm = h2.perm().astype(np.int32)
+    coord = np.ascontiguousarray(Y[:, perm])
+    fp, fi, npt, ni = h2.lists()
+    rank = h2.ranks()
+    adm, inadm = [], []
+    for t in range(h2.n_node):
+        adm += [(t, s) for s in fi[fp[t]:fp[t + 1]] if s > t]
+        inadm += [(t, s) for s in ni[npt[t]:npt[t + 1]] if s > t]
+    adm = np.ascontiguousarray(np.array(adm, np.int32).reshape(-1, 2))
+    inadm = np.ascontiguousarray(np.array(inadm, np.int32).reshape(-1, 2))
+    ncand, so, uo, U, skel = h2.bases()
+    arr = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    keep = [arr(nodes[k]) for k in ("start", "end", "level", "first_child", "n_child", "is_leaf")]
+    h = L.shim_h2_assemble(n, d, h2.max_level, h2.n_node, _p(perm, _i32p), _p(coord, _f64p),
+                           *[_p(a, _i32p) for a in keep], len(adm), _p(adm, _i32p), len(inadm),
+                           _p(inadm, _i32p), _p(arr(rank), _i32p), _p(ncand, _i32p), _p(U, _f64p),
+                           _p(uo, _i32p), _p(skel, _f64p), _p(so, _i32p))
+    grad = np.zeros((d, n))
+    try:
+        Z = L.shim_ref_repulsion(h, _p(Y, _f64p), d, n, _p(grad, _f64p))
+    finally:
+        L.shim_h2_free(h)
+    return -grad, Z

@@ -855,6 +855,21 @@ void ora_h2_ranks(const ora_h2 *h, int *rank)
     if (h->rank) memcpy(rank, h->rank, sizeof(int) * h->n_node);
     else memset(rank, 0, sizeof(int) * h->n_node);
 }
+void ora_h2_bases(const ora_h2 *h, int *ncand, int *skel_off, int *U_off)
+{
+    const int nn = h->n_node;
+    if (h->rank == NULL) {
+        memset(ncand, 0, sizeof(int) * nn);
+        memset(skel_off, 0, sizeof(int) * (nn + 1));
+        memset(U_off, 0, sizeof(int) * (nn + 1));
+        return;
+    }
+    memcpy(ncand, h->ncand, sizeof(int) * nn);
+    memcpy(skel_off, h->skel_off, sizeof(int) * (nn + 1));
+    memcpy(U_off, h->U_off, sizeof(int) * (nn + 1));
+}
+const double *ora_h2_U(const ora_h2 *h) { return h->U; }
+const double *ora_h2_skel(const ora_h2 *h) { return h->skel; }
 
 /* ===================================================================================
  * Whole optimisation phase (reference src/tsne_h2pack.c:1652-2102, sklearn mode)

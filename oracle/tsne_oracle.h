@@ -72,6 +72,13 @@ int  ora_h2_n_near(const ora_h2 *h);
 /* CSR by target node, partners ascending */
 void ora_h2_lists(const ora_h2 *h, int *far_ptr, int *far_idx, int *near_ptr, int *near_idx);
 void ora_h2_ranks(const ora_h2 *h, int *rank);
+/* Bases, for handing the matrix to another product code: per node the candidate rows of U
+ * (a leaf's points, or its children's skeletons in child order), and the offsets of its
+ * skeleton points (skel_off, n_node + 1 entries) and of its U block (U_off, n_node + 1);
+ * U blocks are ncand x rank row-major, skeleton points d coordinates each. */
+void ora_h2_bases(const ora_h2 *h, int *ncand, int *skel_off, int *U_off);
+const double *ora_h2_U(const ora_h2 *h);
+const double *ora_h2_skel(const ora_h2 *h);
 int  ora_h2_n_proxy(int d);
 void ora_h2_proxies(int d, double h, double *out);   /* d x n_proxy, relative to a box centre */
 

@@ -144,6 +144,25 @@ def test_h2_product_within_tolerance(evolved, it):
     assert abs(Z - Ze) < 1e-2 * Ze
 
 
+@needs_ref
+@pytest.mark.parametrize("d,it,leaf", [(2, 20, 100), (2, 300, 50), (3, 150, 100)])
+def test_h2_force_equals_reference_code_on_the_same_matrix(d, it, leaf):
+    """The reference's own compute_repulsive_forces_h2pack (its fused product
+    tsne_h2_matmul.c:225-452, diagonal removal, Z identity and force, tsne_h2pack.c:389-630),
+    compiled from its sources and handed the oracle's H2 matrix (tree, reduced admissible and
+    inadmissible pair lists, bases, skeletons), gives the oracle's product, Z and force to
+    rounding: the oracle's far/near traversal, mixed-level pairs, upward and downward passes
+    and force assembly are the reference's."""
+    X, G, P, _ = problem(3000, seed=1, n_clusters=12, dim=20)
+    Y = O.run(P, O.init_embedding(3000, d, 2), n_iter=it)[0]
+    h = O.H2(Y, leaf_size=leaf, tol=1e-2)
+    Fr, Zr = O.ref_h2_repulsion(h)
+    s, v = h.product()
+    Zo, Fo = O.z_force(Y, s, v)
+    assert abs(Zr - Zo) <= 1e-11 * Zo
+    assert rel2(Fr, Fo) <= 1e-11
+
+
 def test_tree_is_a_partition(evolved):
     h = O.H2(evolved[300], leaf_size=40, tol=1e-2)
     nd = h.nodes()

@@ -103,7 +103,9 @@ TSNE_API tsne_workspace_t *tsne_init(const DTYPE *X, int n_point, int pt_dim, in
 
 /* reference tsne_h2pack.h:196 / src/tsne_h2pack.c:1356-1547. Takes ownership of P (which
  * must come from sparse_matrix_create); uploads P and the initial embedding and builds
- * the first H2 matrix on the device. NULL on bad low_dim or P shape, or a failed build. */
+ * the first H2 matrix on the device. NULL on bad low_dim or P shape, or a failed build;
+ * also NULL, with P left to the caller, for row pointers that do not start at 0 or that
+ * decrease, and for a column index outside [0, n_point) (checked on the host). */
 TSNE_API tsne_workspace_t *tsne_init_with_P(const DTYPE *X, int n_point, int pt_dim, int low_dim,
                                    const tsne_params_t *params, sparse_matrix_t *P);
 

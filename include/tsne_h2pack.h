@@ -196,6 +196,13 @@ TSNE_API int tsne_h2_get_nodes(H2Pack_p h2, int *start, int *end, int *level, in
 TSNE_API int tsne_h2_get_lists(H2Pack_p h2, int *far_ptr, int *far_idx, int *near_ptr, int *near_idx);
 /* per-node skeleton rank (n_node) */
 TSNE_API int tsne_h2_get_ranks(H2Pack_p h2, int *rank);
+/* the bases: node t's U rows are row_off[t] .. row_off[t] + m_t - 1 (m_t = its leaf's points,
+ * or its children's ranks summed, in child order), max_rank floats each, row-major (columns
+ * past the node's rank unused); skel: n_node x max_rank skeleton points of low_dim floats.
+ * row_off has n_node + 1 entries, U n_rows x max_rank. With U == NULL only *n_rows and
+ * *max_rank are set. 0 on success, -1 without a built matrix. */
+TSNE_API int tsne_h2_get_bases(H2Pack_p h2, int *n_rows, int *max_rank, long long *row_off, float *U,
+                               float *skel);
 /* Current device state in the caller's order: Y (low_dim x n_point), and the repulsive
  * force of the last rebuild (low_dim x n_point, NULL to skip) */
 TSNE_API int tsne_get_state(tsne_workspace_t *workspace, DTYPE *Y_out, DTYPE *rep_out, DTYPE *rep_Z);

@@ -448,27 +448,39 @@ def ref_h2_repulsion(h2, Y=None):
     """The reference's compute_repulsive_forces_h2pack (src/tsne_h2pack.c:389-630, with its
     fused product src/tsne_h2_matmul.c:225-452) run on the H2 matrix `h2` that the oracle
     built: returns (F, Z), F (d, n) in the caller's order."""
-    L = ref_lib()
     Y = h2.Y if Y is None else np.ascontiguousarray(Y, dtype=np.float64)
+    ncand, so, uo, U, skel = h2.bases()
+    return ref_h2_repulsion_on(Y, h2.perm(), h2.nodes(), h2.lists(), h2.max_level, h2.ranks(), ncand, U, uo,
+                               skel, so)
+
+
+def ref_h2_repulsion_on(Y, perm, nodes, lists, max_level, rank, ncand, U, U_off, skel, skel_off):
+    """The reference's repulsive force on any H2 matrix given as arrays: perm (tree position
+    -> point), the node table (dict of start, end, level, first_child, n_child, is_leaf), the
+    per-target lists (far_ptr, far_idx, near_ptr, near_idx, both directions of every pair),
+    ranks, and the bases packed as by H2.bases(). Returns (F, Z)."""
+    L = ref_lib()
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
     d, n = Y.shape
-    nodes = h2.nodes()
-    perm = h2.perm().astype(np.int32)
+    perm = np.ascontiguousarray(perm, dtype=np.int32)
     coord = np.ascontiguousarray(Y[:, perm])
-    fp, fi, npt, ni = h2.lists()
-    rank = h2.ranks()
+    fp, fi, npt, ni = lists
+    n_node = len(rank)
     adm, inadm = [], []
-    for t in range(h2.n_node):
+    for t in range(n_node):
         adm += [(t, s) for s in fi[fp[t]:fp[t + 1]] if s > t]
         inadm += [(t, s) for s in ni[npt[t]:npt[t + 1]] if s > t]
     adm = np.ascontiguousarray(np.array(adm, np.int32).reshape(-1, 2))
     inadm = np.ascontiguousarray(np.array(inadm, np.int32).reshape(-1, 2))
-    ncand, so, uo, U, skel = h2.bases()
     arr = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
     keep = [arr(nodes[k]) for k in ("start", "end", "level", "first_child", "n_child", "is_leaf")]
-    h = L.shim_h2_assemble(n, d, h2.max_level, h2.n_node, _p(perm, _i32p), _p(coord, _f64p),
+    rank, ncand, U_off, skel_off = arr(rank), arr(ncand), arr(U_off), arr(skel_off)
+    U, skel = f64(U), f64(skel)
+    h = L.shim_h2_assemble(n, d, int(max_level), n_node, _p(perm, _i32p), _p(coord, _f64p),
                            *[_p(a, _i32p) for a in keep], len(adm), _p(adm, _i32p), len(inadm),
-                           _p(inadm, _i32p), _p(arr(rank), _i32p), _p(ncand, _i32p), _p(U, _f64p),
-                           _p(uo, _i32p), _p(skel, _f64p), _p(so, _i32p))
+                           _p(inadm, _i32p), _p(rank, _i32p), _p(ncand, _i32p), _p(U, _f64p),
+                           _p(U_off, _i32p), _p(skel, _f64p), _p(skel_off, _i32p))
     grad = np.zeros((d, n))
     try:
         Z = L.shim_ref_repulsion(h, _p(Y, _f64p), d, n, _p(grad, _f64p))

@@ -1222,6 +1222,13 @@ int tsne_h2_get_ranks(H2Pack_p h2, int *rank)
     return 0;
 }
 
+int tsne_h2_get_bases(H2Pack_p h2, int *n_rows, int *max_rank, long long *row_off, float *U, float *skel)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2 || n_rows == nullptr || max_rank == nullptr) return -1;
+    if (U != nullptr && (row_off == nullptr || skel == nullptr)) return -1;
+    try { return h2->ws->h2->copy_bases(n_rows, max_rank, row_off, U, skel); } catch (const CudaError &) { return -1; }
+}
+
 int tsne_get_state(tsne_workspace_t *ws, double *Y_out, double *rep_out, double *rep_Z)
 {
     if (ws == nullptr) return -1;

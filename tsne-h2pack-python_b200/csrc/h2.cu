@@ -1057,7 +1057,6 @@ __device__ __forceinline__ void warp_argmax(float &bv, int &bi)
 // y0 = U^T (the leaf's [1 | x] | the children's y0) are summed by all threads in a fixed order.
 constexpr int ID2_THREADS = 128;                  // internal nodes and leaves of 65..128 points
 constexpr int ID2_SMALL = 64;                     // leaves of at most 64 points
-constexpr int ID2_MAX_ROWS = 2 * ID2_THREADS;     // four children of rank MAXR
 constexpr int ID2_DSTRIDE = Dim<2>::MAXR + 1;
 constexpr size_t id2_smem(int threads) { return sizeof(float) * threads * ID2_DSTRIDE; }   // dot products
 
@@ -2073,6 +2072,26 @@ public:
         TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
         if (built_) TSNE_CUDA_CHECK(cudaMemcpy(rank, rank_.p, sizeof(int) * n_node_, cudaMemcpyDeviceToHost));
         else for (int i = 0; i < n_node_; i++) rank[i] = 0;
+    }
+
+    int copy_bases(int *n_rows, int *max_rank, long long *row_off, float *U, float *skel) override
+    {
+        constexpr int MAXR = Dim<D>::MAXR;
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+        if (!built_) return -1;
+        *n_rows = (int)hrows_;
+        *max_rank = MAXR;
+        if (U == nullptr) return 0;
+        TSNE_CUDA_CHECK(cudaMemcpy(row_off, rowoff_.p, sizeof(long long) * (n_node_ + 1), cudaMemcpyDeviceToHost));
+        if (hrows_ > 0)
+            TSNE_CUDA_CHECK(cudaMemcpy(U, U_.p, sizeof(float) * (size_t)hrows_ * MAXR, cudaMemcpyDeviceToHost));
+        std::vector<Vec<D>> sk((size_t)n_node_ * MAXR);
+        TSNE_CUDA_CHECK(cudaMemcpy(sk.data(), skel_.p, sizeof(Vec<D>) * sk.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < sk.size(); i++) {
+            const float *f = reinterpret_cast<const float *>(&sk[i]);   // x, y (, z)
+            for (int k = 0; k < D; k++) skel[i * D + k] = f[k];
+        }
+        return 0;
     }
 
     long long launches() const override { return launches_; }

@@ -41,6 +41,11 @@ public:
                             int *nchild, int *leaf) = 0;
     virtual void copy_lists(int *far_ptr, int *far_idx, int *near_ptr, int *near_idx) = 0;
     virtual void copy_ranks(int *rank) = 0;
+    // the bases: node t's U rows are row_off[t] .. row_off[t] + (its leaf's points, or its
+    // children's ranks summed) - 1, max_rank floats each (columns past the node's rank
+    // unused); skel holds max_rank skeleton points of d floats per node. With U == nullptr
+    // only n_rows (= row_off[n_node]) and max_rank are returned. -1 before a build.
+    virtual int copy_bases(int *n_rows, int *max_rank, long long *row_off, float *U, float *skel) = 0;
     virtual long long launches() const = 0;
     // 1 when a bounded wait of a dependency-ordered launch gave up since the last build
     // (its results are not to be trusted); synchronises the stream

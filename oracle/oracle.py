@@ -375,21 +375,29 @@ def ref_init_embedding(n, d, seed):
 
 
 def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=250,
-            sklearn_compatible=1, nthreads=1, attr_f32=0):
-    """The reference's own tsne_run on its exact-repulsion path (h2_rebuild_freq=999999,
-    i.e. method='exact'); P: symmetric normalised scipy CSR; Y0: (d, n)."""
+            sklearn_compatible=1, nthreads=1, attr_f32=0, h2=False, h2_tol=1e-2, h2_rebuild_freq=3,
+            h2_rebuild_freq_early=10, h2_leaf_size=100, attr_generic=False):
+    """The reference's own tsne_run; P: symmetric normalised scipy CSR; Y0: (d, n).
+
+    h2=False: its exact-repulsion path (h2_rebuild_freq=999999, i.e. method='exact').
+    h2=True: its H2 path, with every H2 matrix built by the oracle behind the H2Pack
+    interface (ref_shim/h2_assemble.c): the reference's rebuild schedule, force reuse,
+    renumbering, fused product, Z identity and force run on the oracle's matrices.
+    attr_generic selects its FP64 attractive pass (TSNE_ATTR_GENERIC=1) instead of the
+    2D single-precision gather."""
     L = ref_lib()
     os.environ["TSNE_ATTR_F32"] = str(attr_f32)
+    os.environ["TSNE_ATTR_GENERIC"] = "1" if attr_generic else "0"
     Y0 = np.ascontiguousarray(Y0, dtype=np.float64)
     d, n = Y0.shape
     prm = _RefParams(n_iter=n_iter, perplexity=30.0,
                      learning_rate=learning_rate or max(n / 12.0, 200.0), momentum=0.8,
                      initial_momentum=0.5, momentum_switch_iter=250, early_exag=early_exag,
-                     early_exag_iter=early_exag_iter, use_vptree=2, h2_tol=1e-4,
-                     h2_rebuild_freq=999999, init_method=1, random_seed=0, verbose=0,
-                     print_freq=50, convergence_tol=1e-5, convergence_patience=300, min_iter=250,
-                     sklearn_compatible=sklearn_compatible, num_threads=nthreads, h2_leaf_size=100,
-                     h2_rebuild_freq_early=999999, init_Y=_p(Y0, _f64p))
+                     early_exag_iter=early_exag_iter, use_vptree=2, h2_tol=h2_tol if h2 else 1e-4,
+                     h2_rebuild_freq=h2_rebuild_freq if h2 else 999999, init_method=1, random_seed=0,
+                     verbose=0, print_freq=50, convergence_tol=1e-5, convergence_patience=300, min_iter=250,
+                     sklearn_compatible=sklearn_compatible, num_threads=nthreads, h2_leaf_size=h2_leaf_size,
+                     h2_rebuild_freq_early=h2_rebuild_freq_early if h2 else 999999, init_Y=_p(Y0, _f64p))
     nnz = P.nnz
     m = L.sparse_matrix_create(n, n, nnz)
     ctypes.memmove(m.contents.row_ptr, np.ascontiguousarray(P.indptr, np.int32).ctypes.data, 4 * (n + 1))

@@ -3,13 +3,13 @@
  *
  * The reference's optimisation loop (src/tsne_h2pack.c, src/tsne_h2_matmul.c,
  * src/tsne_reorder.c, src/tsne_utils.c) is compiled unmodified against this
- * header to obtain the reference's OWN exact-repulsion path (the skip_h2 branch,
- * tsne_h2pack.c:874-892, and the direct O(N^2) branch, tsne_h2pack.c:404-491).
- * The H2Pack git submodule is empty in the reference checkout, so nothing here is
- * H2Pack code: the struct below only declares the member names the reference
+ * header. The H2Pack git submodule is empty in the reference checkout, so nothing
+ * here is H2Pack code: the struct below only declares the member names the reference
  * sources read (tsne_h2pack.c:107-136, 772-953; tsne_h2_matmul.c:196-249) so that
- * they compile, and h2pack_stub.c reports a tree too shallow for an H2 matrix
- * (max_level 0), which routes every iteration through the reference's direct path.
+ * they compile, and h2_assemble.c fills them with the H2 matrix the oracle builds
+ * (oracle/tsne_oracle.c). The reference's own loop, rebuild schedule, renumbering,
+ * fused product, Z identity and force then run on the oracle's matrices; for
+ * N < 2000 or a tree of at most two levels they take their direct O(N^2) branch.
  */
 #ifndef ORACLE_REF_SHIM_H2PACK_H
 #define ORACLE_REF_SHIM_H2PACK_H
@@ -54,6 +54,11 @@ typedef struct {
     shim_krnl_eval_fptr krnl_eval;
     const void *krnl_param;
     double timers[9];
+    /* shim only: the oracle's matrix behind H2P_partition_points / H2P_build, and the
+     * relative tolerance H2P_init received */
+    void *ora;
+    double qr_tol;
+    const DTYPE *coord_src;   /* the points the partition saw (the caller's order) */
 } shim_h2pack_t;
 typedef shim_h2pack_t *H2Pack_p;
 

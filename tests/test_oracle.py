@@ -163,6 +163,24 @@ def test_h2_force_equals_reference_code_on_the_same_matrix(d, it, leaf):
     assert rel2(Fr, Fo) <= 1e-11
 
 
+@needs_ref
+@pytest.mark.parametrize("d,n_iter,tol_y,tol_kl", [(2, 25, 1e-9, 1e-11), (2, 40, 1e-4, 1e-8), (3, 30, 1e-5, 1e-9)])
+def test_reference_loop_on_oracle_matrices_equals_oracle_run(d, n_iter, tol_y, tol_kl):
+    """The reference's own tsne_run on its H2 path (tsne_h2pack.c:1652-2102: rebuild every
+    iteration below 20 and every 10 after, force and Z reuse between rebuilds, renumbering at
+    the first rebuild >= 30, its update, centring and KL), with every H2 matrix built by the
+    oracle behind the H2Pack interface (ref_shim/h2_assemble.c) and its FP64 attractive pass,
+    follows the oracle's own run: to rounding through 25 iterations, and after the
+    renumbering at iteration 30 (40 iterations) to the ~2x-per-iteration growth of rounding
+    differences that t-SNE shows, KL to 1e-8."""
+    X, G, P, _ = problem(5000, seed=1, n_clusters=12, dim=20)
+    Y0 = O.init_embedding(P.shape[0], d, 4)
+    Yr, klr = O.ref_run(P, Y0, n_iter, h2=True, attr_generic=True, nthreads=4)
+    Yo, klo = O.run(P, Y0, n_iter=n_iter)
+    assert rel(Yr, Yo) < tol_y
+    assert abs(klr - klo) <= tol_kl * abs(klo)
+
+
 def test_tree_is_a_partition(evolved):
     h = O.H2(evolved[300], leaf_size=40, tol=1e-2)
     nd = h.nodes()

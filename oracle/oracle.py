@@ -376,7 +376,7 @@ def ref_init_embedding(n, d, seed):
 
 def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=250,
             sklearn_compatible=1, nthreads=1, attr_f32=0, h2=False, h2_tol=1e-2, h2_rebuild_freq=3,
-            h2_rebuild_freq_early=10, h2_leaf_size=100, attr_generic=False):
+            h2_rebuild_freq_early=10, h2_leaf_size=100, attr_generic=False, profile=None):
     """The reference's own tsne_run; P: symmetric normalised scipy CSR; Y0: (d, n).
 
     h2=False: its exact-repulsion path (h2_rebuild_freq=999999, i.e. method='exact').
@@ -384,7 +384,8 @@ def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=
     interface (ref_shim/h2_assemble.c): the reference's rebuild schedule, force reuse,
     renumbering, fused product, Z identity and force run on the oracle's matrices.
     attr_generic selects its FP64 attractive pass (TSNE_ATTR_GENERIC=1) instead of the
-    2D single-precision gather."""
+    2D single-precision gather. profile: a path; the reference writes its per-iteration
+    stage times there (tsne_write_profiling_data's CSV), read back by ref_profile_csv."""
     L = ref_lib()
     os.environ["TSNE_ATTR_F32"] = str(attr_f32)
     os.environ["TSNE_ATTR_GENERIC"] = "1" if attr_generic else "0"
@@ -397,7 +398,9 @@ def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=
                      h2_rebuild_freq=h2_rebuild_freq if h2 else 999999, init_method=1, random_seed=0,
                      verbose=0, print_freq=50, convergence_tol=1e-5, convergence_patience=300, min_iter=250,
                      sklearn_compatible=sklearn_compatible, num_threads=nthreads, h2_leaf_size=h2_leaf_size,
-                     h2_rebuild_freq_early=h2_rebuild_freq_early if h2 else 999999, init_Y=_p(Y0, _f64p))
+                     h2_rebuild_freq_early=h2_rebuild_freq_early if h2 else 999999, init_Y=_p(Y0, _f64p),
+                     enable_profiling=1 if profile else 0,
+                     profiling_output_file=str(profile).encode() if profile else None)
     nnz = P.nnz
     m = L.sparse_matrix_create(n, n, nnz)
     ctypes.memmove(m.contents.row_ptr, np.ascontiguousarray(P.indptr, np.int32).ctypes.data, 4 * (n + 1))
@@ -415,6 +418,16 @@ def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=
     finally:
         L.tsne_destroy(ws)
     return Y, kl_val
+
+
+def ref_profile_csv(path):
+    """Per-iteration stage times (seconds) from the reference's profiling CSV: a dict of
+    arrays keyed by its columns (p_matvec = attractive pass, h2_rebuild, h2_matvec_s = fused
+    product, z_computation, gradient = update, other)."""
+    rows = [ln.strip().split(",") for ln in Path(path).read_text().splitlines()
+            if ln and not ln.startswith("#")]
+    head, body = rows[0], [r for r in rows[1:] if len(r) == len(rows[0])]
+    return {k: np.array([float(r[i]) for r in body]) for i, k in enumerate(head)}
 
 
 class Runner:

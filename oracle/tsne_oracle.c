@@ -237,15 +237,6 @@ static uint64_t ora_interleave(const uint32_t *q, int d, int L)
     return key;
 }
 
-static int ora_key_cmp(const void *a, const void *b, void *keys_)
-{
-    const uint64_t *keys = (const uint64_t *)keys_;
-    const int ia = *(const int *)a, ib = *(const int *)b;
-    if (keys[ia] < keys[ib]) return -1;
-    if (keys[ia] > keys[ib]) return 1;
-    return (ia > ib) - (ia < ib);   /* stable: original order for equal keys */
-}
-
 /* Node admissibility on integer coordinates: with w = box width in finest cells and
  * 2*centre = 2*ix*w + w, boxes t, s are well separated iff
  *   max_k |2c_t - 2c_s| >= w_t + w_s + 2 min(w_t, w_s)
@@ -280,19 +271,47 @@ static void iv_push(ora_ivec *v, int x)
 }
 static int ora_int_cmp(const void *a, const void *b) { const int x = *(const int *)a, y = *(const int *)b; return (x > y) - (x < y); }
 
-static int ora_build_tree(ora_h2 *h, const double *Y)
+/* Stable LSD radix sort of perm (initially 0..n-1) by keys[perm[i]] over the low `bits`
+ * bits: equal keys keep index order, as a comparison sort with the index as tie-break. */
+static void ora_radix_sort(int *perm, const uint64_t *keys, int n, int bits)
+{
+    int *tmp = (int *)malloc(sizeof(int) * (size_t)n);
+    uint64_t *kv = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)n);
+    uint64_t *kt = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)n);
+    for (int i = 0; i < n; i++) kv[i] = keys[perm[i]];
+    for (int shift = 0; shift < bits; shift += 8) {
+        size_t cnt[257] = {0};
+        for (int i = 0; i < n; i++) cnt[((kv[i] >> shift) & 255u) + 1]++;
+        for (int b = 0; b < 256; b++) cnt[b + 1] += cnt[b];
+        for (int i = 0; i < n; i++) {
+            const size_t o = cnt[(kv[i] >> shift) & 255u]++;
+            tmp[o] = perm[i];
+            kt[o] = kv[i];
+        }
+        memcpy(perm, tmp, sizeof(int) * (size_t)n);
+        memcpy(kv, kt, sizeof(uint64_t) * (size_t)n);
+    }
+    free(tmp); free(kv); free(kt);
+}
+
+static int ora_build_tree(ora_h2 *h, const double *Y, int nthreads)
 {
     const int n = h->n, d = h->d, L = h->L;
+    const int nth = nthreads > 0 ? nthreads : 1;
     double lo[3], hi[3];
-    for (int k = 0; k < d; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
     int bad = 0;
-    for (int k = 0; k < d; k++)
+    for (int k = 0; k < d; k++) {
+        double l0 = INFINITY, h0 = -INFINITY;
+        int b0 = 0;
+        #pragma omp parallel for num_threads(nth) reduction(min:l0) reduction(max:h0) reduction(|:b0)
         for (int i = 0; i < n; i++) {
             const double y = Y[(size_t)k * n + i];
-            if (!isfinite(y)) { bad = 1; continue; }
-            if (y < lo[k]) lo[k] = y;
-            if (y > hi[k]) hi[k] = y;
+            if (!isfinite(y)) { b0 = 1; continue; }
+            if (y < l0) l0 = y;
+            if (y > h0) h0 = y;
         }
+        lo[k] = l0; hi[k] = h0; bad |= b0;
+    }
     if (bad) return -1;
     double ext = 0.0, ctr[3];
     for (int k = 0; k < d; k++) {
@@ -309,6 +328,7 @@ static int ora_build_tree(ora_h2 *h, const double *Y)
 
     uint32_t *q0 = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)n * d);
     uint64_t *k0 = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)n);
+    #pragma omp parallel for num_threads(nth) schedule(static)
     for (int i = 0; i < n; i++) {
         for (int k = 0; k < d; k++) {
             const double t = (Y[(size_t)k * n + i] - h->corner[k]) / cell;
@@ -320,7 +340,8 @@ static int ora_build_tree(ora_h2 *h, const double *Y)
         k0[i] = ora_interleave(q0 + (size_t)i * d, d, L);
     }
     for (int i = 0; i < n; i++) h->perm[i] = i;
-    qsort_r(h->perm, (size_t)n, sizeof(int), ora_key_cmp, k0);
+    ora_radix_sort(h->perm, k0, n, d * L);
+    #pragma omp parallel for num_threads(nth) schedule(static)
     for (int t = 0; t < n; t++) {
         const int i = h->perm[t];
         h->keys[t] = k0[i];
@@ -414,15 +435,19 @@ static void ora_classify_leaf(const ora_h2 *h, int t, int c, ora_ivec *far, ora_
     }
 }
 
-static void ora_build_lists(ora_h2 *h)
+static void ora_build_lists(ora_h2 *h, int nthreads)
 {
+    const int nth = nthreads > 0 ? nthreads : 1;
     const int nn = h->n_node;
     ora_ivec *Nset = (ora_ivec *)calloc((size_t)nn, sizeof(ora_ivec));
     ora_ivec *far = (ora_ivec *)calloc((size_t)nn, sizeof(ora_ivec));
     ora_ivec *near = (ora_ivec *)calloc((size_t)nn, sizeof(ora_ivec));
     if (h->leaf[0]) iv_push(&near[0], 0);
     else iv_push(&Nset[0], 0);
+    /* the targets of a level depend only on their parents' sets: one level at a time, the
+     * targets of a level in parallel (each writes only its own sets) */
     for (int l = 1; l <= h->max_level; l++) {
+        #pragma omp parallel for num_threads(nth) schedule(dynamic, 16)
         for (int t = h->lvl_begin[l]; t < h->lvl_begin[l + 1]; t++) {
             const int p = h->parent[t];
             for (int a = 0; a < Nset[p].n; a++) {
@@ -453,6 +478,7 @@ static void ora_build_lists(ora_h2 *h)
     }
     h->far_idx = (int *)malloc(sizeof(int) * (h->far_ptr[nn] + 1));
     h->near_idx = (int *)malloc(sizeof(int) * (h->near_ptr[nn] + 1));
+    #pragma omp parallel for num_threads(nth) schedule(dynamic, 64)
     for (int t = 0; t < nn; t++) {
         if (far[t].n) {
             qsort(far[t].a, far[t].n, sizeof(int), ora_int_cmp);
@@ -680,8 +706,8 @@ ora_h2 *ora_h2_build(const double *Y, int n, int d, int leaf_size, double tol, i
     h->keys = (uint64_t *)malloc(sizeof(uint64_t) * n);
     h->perm = (int *)malloc(sizeof(int) * n);
     h->q = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)n * d);
-    if (ora_build_tree(h, Y) != 0) { if (status) *status = -1; ora_h2_free(h); return NULL; }
-    ora_build_lists(h);
+    if (ora_build_tree(h, Y, nthreads) != 0) { if (status) *status = -1; ora_h2_free(h); return NULL; }
+    ora_build_lists(h, nthreads);
     if (h->max_level <= 2) { if (status) *status = 1; return h; }
     ora_build_bases(h, Y, nthreads);
     return h;

@@ -64,6 +64,8 @@ def lib():
         L.ora_conditional_P.argtypes = [_f64p, _i32p, ctypes.c_int, ctypes.c_double, _f64p, ctypes.c_int]
         L.ora_init_embedding.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, ctypes.c_uint]
         L.ora_exact_sv.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, _f64p, _f64p, ctypes.c_int]
+        L.ora_exact_rows.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, _f64p, _f64p,
+                                     ctypes.c_int]
         L.ora_z_force.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, _f64p, _f64p, _f64p]
         L.ora_z_force.restype = ctypes.c_double
         L.ora_attractive.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p,
@@ -134,6 +136,18 @@ def exact_sv(Y, nthreads=None):
     d, n = Y.shape
     s = np.zeros(n); v = np.zeros((d, n))
     lib().ora_exact_sv(_p(Y, _f64p), n, d, _p(s, _f64p), _p(v, _f64p), nthreads or nthreads_default())
+    return s, v
+
+
+def exact_rows(Y, rows, nthreads=None):
+    """Exact off-diagonal sums for the points `rows` only: s (m,), v (d, m)."""
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    d, n = Y.shape
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    m = len(rows)
+    s = np.zeros(m); v = np.zeros((d, m))
+    lib().ora_exact_rows(_p(Y, _f64p), n, d, _p(rows, _i32p), m, _p(s, _f64p), _p(v, _f64p),
+                         nthreads or nthreads_default())
     return s, v
 
 

@@ -136,6 +136,25 @@ void ora_exact_sv(const double *Y, int n, int d, double *s, double *v, int nthre
     }
 }
 
+void ora_exact_rows(const double *Y, int n, int d, const int *rows, int m, double *s, double *v, int nthreads)
+{
+    #pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads > 0 ? nthreads : 1)
+    for (int r = 0; r < m; r++) {
+        const int i = rows[r];
+        double si = 0.0, vi[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < n; j++) {
+            if (j == i) continue;
+            double r2 = 0.0;
+            for (int k = 0; k < d; k++) { const double df = Y[(size_t)k * n + i] - Y[(size_t)k * n + j]; r2 += df * df; }
+            const double w = ora_kernel(r2);
+            si += w;
+            for (int k = 0; k < d; k++) vi[k] += w * Y[(size_t)k * n + j];
+        }
+        s[r] = si;
+        for (int k = 0; k < d; k++) v[(size_t)k * m + r] = vi[k];
+    }
+}
+
 double ora_z_force(const double *Y, int n, int d, const double *s, const double *v, double *F)
 {
     double t1 = 0.0, t2 = 0.0, t3 = 0.0;

@@ -40,6 +40,8 @@ void ora_init_embedding(double *Y, int n, int d, unsigned int seed);
 
 /* ---- per-iteration pieces (Y is d x n, dimension-major) ---- */
 void   ora_exact_sv(const double *Y, int n, int d, double *s, double *v, int nthreads);
+/* the same sums for the m points rows[]: s (m), v (d x m) */
+void   ora_exact_rows(const double *Y, int n, int d, const int *rows, int m, double *s, double *v, int nthreads);
 double ora_z_force(const double *Y, int n, int d, const double *s, const double *v, double *F);
 void   ora_attractive(int n, int d, const int *rp, const int *ci, const double *pv,
                       const double *Y, double exag, double *attr, int nthreads);

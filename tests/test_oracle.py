@@ -181,6 +181,43 @@ def test_reference_loop_on_oracle_matrices_equals_oracle_run(d, n_iter, tol_y, t
     assert abs(klr - klo) <= tol_kl * abs(klo)
 
 
+def _zipf_cloud(n, d, spread, seed):
+    """n points in d dimensions: 100 Gaussian clusters of Zipf(1.1) sizes (a stand-in for a
+    converged embedding of the benchmark's mixture), rounded to float32."""
+    rng = np.random.default_rng(seed)
+    w = np.arange(1, 101) ** -1.1
+    cnt = rng.multinomial(n, w / w.sum())
+    cen = rng.normal(0, spread, (100, d))
+    sd = rng.uniform(1, 4, (100, d))
+    lab = np.repeat(np.arange(100), cnt)
+    Y = (cen[lab] + sd[lab] * rng.standard_normal((n, d))).T
+    return np.ascontiguousarray(Y).astype(np.float32).astype(np.float64), rng
+
+
+@pytest.mark.parametrize("n,d,tol", [(1_000_000, 2, 1e-2), (500_000, 3, 3e-2)])
+def test_h2_accuracy_at_full_size(n, d, tol):
+    """At the benchmark sizes (1M points in 2D with h2_tol 1e-2; 500K in 3D with 3e-2), the H2
+    sums of 400 random points against their exact FP64 sums over all points: s and v within
+    tol / 5, the force numerator y s - v within tol. (Exact sums for every point are out of
+    reach at this size; the sampled rows check the same property.)"""
+    Y, rng = _zipf_cloud(n, d, 40.0 if d == 2 else 25.0, 7 + d)
+    h = O.H2(Y, leaf_size=100, tol=tol)
+    s, v = h.product()
+    rows = np.sort(rng.choice(n, 400, replace=False))
+    se, ve = O.exact_rows(Y, rows)
+    assert rel2(s[rows], se) < tol / 5 and rel2(v[:, rows], ve) < tol / 5
+    assert rel2(Y[:, rows] * s[rows] - v[:, rows], Y[:, rows] * se - ve) < tol
+
+
+def test_exact_rows_equal_exact_sums():
+    Y = O.init_embedding(3000, 3, 5) * 1e3
+    rows = np.array([0, 17, 1500, 2999], dtype=np.int32)
+    s, v = O.exact_sv(Y)
+    sr, vr = O.exact_rows(Y, rows)
+    np.testing.assert_array_equal(sr, s[rows])
+    np.testing.assert_array_equal(vr, v[:, rows])
+
+
 def test_tree_is_a_partition(evolved):
     h = O.H2(evolved[300], leaf_size=40, tol=1e-2)
     nd = h.nodes()

@@ -224,9 +224,10 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
 }
 
-// The same step with the Y gathers served from shared memory (TSNE_ATTR_WINDOW=1; off by
-// default). One CTA per SM owns a contiguous range of rows holding an equal share of P's
-// entries and stages the window of Y centred on it (win_pts points, 128 KB) once; a column
+// The same step with the Y gathers served from shared memory (TSNE_ATTR_WINDOW=1 or 2; off by
+// default). One CTA per SM (form 2: two) owns a contiguous range of rows holding an equal
+// share of P's entries and stages the window of Y centred on it (WINP points: 128 KB, form 2
+// 64 KB) once; a column
 // inside the window is read from shared memory, one outside it through L1/L2. After the
 // renumbering in tree order about three quarters of a point's neighbours lie inside a
 // 16K-point window around it (200K-point 2D embedding of the benchmark mixture), so most
@@ -254,14 +255,14 @@ __device__ __forceinline__ int first_row_at(const int *__restrict__ rp, int n, l
     return lo;
 }
 
-template <int D, int MODE>
-__global__ void __launch_bounds__(WIN_THREADS, 1)
+template <int D, int MODE, int WINP, int MINB>
+__global__ void __launch_bounds__(WIN_THREADS, MINB)
 k_attr_window(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
               const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
               Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
               float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
 {
-    constexpr int WIN = win_pts<D>();
+    constexpr int WIN = WINP;
     constexpr int NH = WIN_THREADS / 16;   // half-warps per CTA
     extern __shared__ __align__(16) unsigned char win_raw[];
     Vec<D> *win = reinterpret_cast<Vec<D> *>(win_raw);
@@ -689,30 +690,56 @@ inline int ew_grid(int n) { int g = ceil_div(n, EW_BLOCK); return g < 1 ? 1 : (g
 // ---------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------
-// The shared-memory window form of the attractive step (k_attr_window) is taken while every
-// CTA's row range fits in half a window, when TSNE_ATTR_WINDOW=1; all three modes and the
-// centring follow the same rule, so a step's kernels always agree on the row split.
+// The shared-memory window forms of the attractive step (k_attr_window), chosen by
+// TSNE_ATTR_WINDOW: 1, one CTA per SM with a 128 KB window; 2 (2D; 3D takes form 1, its
+// update spills at 32 registers), two CTAs per SM with 64 KB windows (at most 32 registers
+// per thread, so twice the resident warps). A form is taken
+// while the average CTA's row range fits in half its window; all three modes and the
+// centring follow the same rule, so a step's kernels always agree on the row split. 0 (the
+// default): k_attr_update.
 template <int D>
-bool use_window(int n)
+int window_form(int n)
 {
-    static const bool on = [] {
+    static const int form = [] {
         const char *e = getenv("TSNE_ATTR_WINDOW");
-        return e != nullptr && atoi(e) != 0;
+        const int v = e != nullptr ? atoi(e) : 0;
+        return (v == 1 || v == 2) ? v : 0;
     }();
-    return on && ceil_div(n, WIN_GRID) <= win_pts<D>() / 2;
+    const int f = (D == 3 && form == 2) ? 1 : form;
+    if (f == 0) return 0;
+    return ceil_div(n, f * WIN_GRID) <= win_pts<D>() / f / 2 ? f : 0;
+}
+template <int D>
+int attr_blocks(int n)
+{
+    const int form = window_form<D>(n);
+    return form == 0 ? ROW_GRID : form * WIN_GRID;
+}
+template <int D, int MODE, int FORM>
+void launch_window_form(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
+                        void *Ynext, void *uY, void *gains, const void *rep, const int *rep_flag, float exag4,
+                        float mom, float lr, double *partials, void *attr)
+{
+    constexpr int WINP = win_pts<D>() / FORM;
+    constexpr size_t smem = MODE == ATTR_UPDATE ? 0 : sizeof(Vec<D>) * (size_t)WINP;
+    static const cudaError_t attr_set = cudaFuncSetAttribute(k_attr_window<D, MODE, WINP, FORM>,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    (void)attr_set;
+    k_attr_window<D, MODE, WINP, FORM><<<FORM * WIN_GRID, WIN_THREADS, smem, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains, (const Vec<D> *)rep,
+        rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
 }
 template <int D, int MODE>
 void launch_window(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
                    void *Ynext, void *uY, void *gains, const void *rep, const int *rep_flag, float exag4, float mom,
                    float lr, double *partials, void *attr)
 {
-    constexpr size_t smem = MODE == ATTR_UPDATE ? 0 : sizeof(Vec<D>) * (size_t)win_pts<D>();
-    static const cudaError_t attr_set =
-        cudaFuncSetAttribute(k_attr_window<D, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    (void)attr_set;
-    k_attr_window<D, MODE><<<WIN_GRID, WIN_THREADS, smem, st>>>(
-        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains, (const Vec<D> *)rep,
-        rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+    if (window_form<D>(n) == 1)
+        launch_window_form<D, MODE, 1>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                       partials, attr);
+    else
+        launch_window_form<D, MODE, 2>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                       partials, attr);
 }
 
 template <int D>
@@ -720,7 +747,7 @@ void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, c
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
                         const int *rep_flag, float exag4, float mom, float lr, double *partials)
 {
-    if (use_window<D>(n)) {
+    if (window_form<D>(n) != 0) {
         launch_window<D, ATTR_FUSED>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
                                      partials, nullptr);
         return;
@@ -733,7 +760,7 @@ template <int D>
 void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
                       void *attr)
 {
-    if (use_window<D>(n)) {
+    if (window_form<D>(n) != 0) {
         launch_window<D, ATTR_GRAD>(st, n, rp, col, val, Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f,
                                     0.f, nullptr, attr);
         return;
@@ -747,7 +774,7 @@ void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Y
                    const void *rep, const int *rep_flag, const void *attr, float exag4, float mom, float lr,
                    double *partials)
 {
-    if (use_window<D>(n)) {
+    if (window_form<D>(n) != 0) {
         launch_window<D, ATTR_UPDATE>(st, n, rp, nullptr, nullptr, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom,
                                       lr, partials, const_cast<void *>(attr));
         return;
@@ -761,7 +788,7 @@ template <int D>
 void launch_center(cudaStream_t st, int n, const void *Ynext, void *Ycur, const double *partials,
                    DevScalars *sc, const void *, double *)
 {
-    const int nblk = use_window<D>(n) ? WIN_GRID : ROW_GRID;
+    const int nblk = attr_blocks<D>(n);
     k_center<D><<<ew_grid(n), RED_BLOCK, 0, st>>>(n, (const Vec<D> *)Ynext, (Vec<D> *)Ycur, partials, nblk, sc);
 }
 

@@ -722,8 +722,15 @@ void launch_window_form(cudaStream_t st, int n, const int *rp, const int *col, c
 {
     constexpr int WINP = win_pts<D>() / FORM;
     constexpr size_t smem = MODE == ATTR_UPDATE ? 0 : sizeof(Vec<D>) * (size_t)WINP;
-    static const cudaError_t attr_set = cudaFuncSetAttribute(k_attr_window<D, MODE, WINP, FORM>,
-                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the window's shared memory, and (two CTAs per SM) a carve-out that holds both windows
+    static const cudaError_t attr_set =
+        FORM == 2 ? (cudaFuncSetAttribute(k_attr_window<D, MODE, WINP, FORM>,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared),
+                     cudaFuncSetAttribute(k_attr_window<D, MODE, WINP, FORM>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
+                  : cudaFuncSetAttribute(k_attr_window<D, MODE, WINP, FORM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     (void)attr_set;
     k_attr_window<D, MODE, WINP, FORM><<<FORM * WIN_GRID, WIN_THREADS, smem, st>>>(
         n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains, (const Vec<D> *)rep,

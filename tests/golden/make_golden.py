@@ -2,10 +2,10 @@
 """Generate the golden vectors of tests/golden/ from the reference's own code.
 
 The reference's C sources (src/tsne_utils.c, src/tsne_h2pack.c, ...) are compiled unmodified
-into oracle/_ref/libtsne_ref.so by `make -C oracle ref`; with the H2Pack stub of oracle/ref_shim
-every tree is shallow, so tsne_run takes the reference's exact-repulsion branch
-(src/tsne_h2pack.c:874-892, the method='exact' path). This script drives that library the way
-the reference's Python backend does and stores its outputs:
+into oracle/_ref/libtsne_ref.so by `make -C oracle ref`. The fixtures use 400 points and
+method='exact' (h2_rebuild_freq 999999), so tsne_run takes the reference's exact-repulsion
+branch (src/tsne_h2pack.c:404-491) and no H2 matrix is involved. This script drives that
+library the way the reference's Python backend does and stores its outputs:
 
   init_*      initialize_embedding (src/tsne_utils.c:1111-1150), glibc srand / Box-Muller
   cond_P      compute_P_from_knn_distances (src/tsne_utils.c:952-1105) on a stored k-NN graph

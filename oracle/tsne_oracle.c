@@ -573,6 +573,18 @@ void ora_h2_proxies(int d, double h, double *out)
     }
 }
 
+/* Dot product in four interleaved partial sums (p mod 4), joined in a fixed order: the
+ * same result on every run, and a loop the compiler vectorises. */
+static inline double ora_dot(const double *x, const double *y, int np)
+{
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    int p = 0;
+    for (; p + 4 <= np; p += 4)
+        for (int k = 0; k < 4; k++) acc[k] += x[p + k] * y[p + k];
+    for (; p < np; p++) acc[0] += x[p] * y[p];
+    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
 /* ID of the m x np matrix A (row-major). Returns the rank r; sel[0..r) = selected rows
  * (in pivot order); U (m x r, row-major) with A ~= U A[sel, :]. */
 static int ora_id(double *A, int m, int np, double tol, int max_rank, int *sel, double *U)
@@ -583,9 +595,7 @@ static int ora_id(double *A, int m, int np, double tol, int max_rank, int *sel, 
     double *R = (double *)calloc((size_t)max_rank * m, sizeof(double));   /* R[k][j], j in pivoted order */
     for (int i = 0; i < m; i++) {
         piv[i] = i;
-        double s = 0.0;
-        for (int p = 0; p < np; p++) s += A[(size_t)i * np + p] * A[(size_t)i * np + p];
-        nrm[i] = s;
+        nrm[i] = ora_dot(A + (size_t)i * np, A + (size_t)i * np, np);
     }
     double n0 = 0.0;
     for (int i = 0; i < m; i++) if (nrm[i] > n0) n0 = nrm[i];
@@ -606,23 +616,17 @@ static int ora_id(double *A, int m, int np, double tol, int max_rank, int *sel, 
             { const double t = nrm[r]; nrm[r] = nrm[best]; nrm[best] = t; }
             for (int k = 0; k < r; k++) { const double t = R[(size_t)k * m + r]; R[(size_t)k * m + r] = R[(size_t)k * m + best]; R[(size_t)k * m + best] = t; }
         }
-        double s = 0.0;
-        for (int p = 0; p < np; p++) s += A[(size_t)r * np + p] * A[(size_t)r * np + p];
-        const double rr = sqrt(s);
+        const double *q = A + (size_t)r * np;
+        const double rr = sqrt(ora_dot(q, q, np));
         R[(size_t)r * m + r] = rr;
         const double inv = 1.0 / rr;
         for (int p = 0; p < np; p++) A[(size_t)r * np + p] *= inv;   /* q_r */
         for (int i = r + 1; i < m; i++) {
-            double dot = 0.0;
-            for (int p = 0; p < np; p++) dot += A[(size_t)r * np + p] * A[(size_t)i * np + p];
+            double *a = A + (size_t)i * np;
+            const double dot = ora_dot(q, a, np);
             R[(size_t)r * m + i] = dot;
-            double s2 = 0.0;
-            for (int p = 0; p < np; p++) {
-                const double v = A[(size_t)i * np + p] - dot * A[(size_t)r * np + p];
-                A[(size_t)i * np + p] = v;
-                s2 += v * v;
-            }
-            nrm[i] = s2;
+            for (int p = 0; p < np; p++) a[p] -= dot * q[p];
+            nrm[i] = ora_dot(a, a, np);
         }
         r++;
     }

@@ -12,10 +12,12 @@ init='random'. A step is one whole optimisation phase (tsne_run) on that input.
           tsne_init_with_P (upload of P and Y0, first H2 build), tsne_run, tsne_get_embedding,
           compute_kl_divergence, tsne_destroy
   roofline  the attractive pass fused with the update (the kernel launched every iteration)
-  cpu_baseline  the CPU oracle (C/OpenMP port of the path) on a bounded sample, all host cores
+  cpu_baseline  the reference's own tsne_run (compiled from its sources in oracle/_ref) on a
+          bounded sample, all host cores; H2Pack's partition and bases, which are absent, are
+          the oracle's restatement behind the H2Pack interface (kind "reference"). Without
+          oracle/_ref, the oracle port (kind "port").
 
---impl reference times the reference path on the host cores instead (the oracle port: the
-reference's own H2 path cannot be built, its H2Pack dependency being absent).
+--impl reference times that same CPU path as its own line.
 Multi-GPU (torchrun): every rank runs its own replica of the workload (no collective on the
 data path); value is the slowest rank's time.
 """

@@ -122,6 +122,30 @@ def test_h2_lists_cover_every_pair_once(evolved, it):
     assert cover.min() == 1 and cover.max() == 1
 
 
+@pytest.mark.parametrize("name", ["3D gaussian", "3D clusters", "2D coincident block"])
+def test_h2_lists_cover_every_pair_once_more_shapes(name):
+    """The same cover property in 3D and with a block of coincident points (a leaf at the key
+    depth holding more than leaf_size points)."""
+    rng = np.random.default_rng(3)
+    if name == "3D gaussian":
+        Y, leaf = rng.normal(size=(3, 2500)), 40
+    elif name == "3D clusters":
+        Y, leaf = rng.normal(size=(3, 2500)) * 1e-2 + rng.integers(0, 4, size=(3, 2500)), 40
+    else:
+        Y, leaf = rng.normal(size=(2, 2500)), 40
+        Y[:, 100:260] = 0.5
+    h = O.H2(Y, leaf_size=leaf, tol=1e-2)
+    nd = h.nodes()
+    fp, fi, np_, ni = h.lists()
+    n = Y.shape[1]
+    cover = np.zeros((n, n), dtype=np.int32)
+    for ptr, idx in ((fp, fi), (np_, ni)):
+        for t in range(h.n_node):
+            for s in idx[ptr[t]:ptr[t + 1]]:
+                cover[nd["start"][t]:nd["end"][t], nd["start"][s]:nd["end"][s]] += 1
+    assert cover.min() == 1 and cover.max() == 1
+
+
 @pytest.mark.parametrize("it", [20, 300])
 def test_h2_lists_symmetric(evolved, it):
     h = O.H2(evolved[it], leaf_size=50, tol=1e-2)

@@ -71,7 +71,7 @@ class FAISSKNN(_KNN):
             import faiss  # noqa: F401
         except ImportError as e:
             raise ImportError("knn_method='faiss' needs the faiss package") from e
-        raise NotImplementedError("knn_method='faiss' is not provided by this build; use 'exact'")
+        raise NotImplementedError("knn_method='faiss' is not available in this package; use 'exact'")
 
 
 class AnnoyKNN(_KNN):
@@ -82,7 +82,7 @@ class AnnoyKNN(_KNN):
             import annoy  # noqa: F401
         except ImportError as e:
             raise ImportError("knn_method='annoy' needs the annoy package") from e
-        raise NotImplementedError("knn_method='annoy' is not provided by this build; use 'exact'")
+        raise NotImplementedError("knn_method='annoy' is not available in this package; use 'exact'")
 
 
 _METHODS = {c.name: c for c in (ExactKNN, BallTreeKNN, PyNNDescentKNN, FAISSKNN, AnnoyKNN)}

@@ -135,6 +135,17 @@ def test_server_rejects_bad_arguments_without_a_device():
     assert lib.tsne_server_pending(None) == -1
 
 
+def test_embedding_server_fails_loudly_without_a_device():
+    """The Python server wrapper raises when the engine cannot create a server (here: no CUDA
+    device), rather than falling back to anything."""
+    import torch
+    from tsne_h2pack.serving import EmbeddingServer
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(RuntimeError):
+        EmbeddingServer(max_concurrent=2, hbm_budget_gb=1.0)
+
+
 @pytest.mark.parametrize("case", ["first_not_zero", "decreasing"])
 def test_init_rejects_bad_row_pointers_before_the_device(case, capfd):
     """tsne_init_with_P checks P's row pointers on the host before it creates any device state

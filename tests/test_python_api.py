@@ -61,3 +61,15 @@ def test_precomputed_graph_checks():
         TSNE(metric="precomputed", perplexity=9, init="random").fit_transform(G)   # 9 neighbours <= 9
     with pytest.raises(ValueError):
         t.fit_transform(csr_matrix(-(np.ones((10, 10)) - np.eye(10))))            # negative distances
+
+
+def test_no_cpu_fallback_without_a_device():
+    """Without a CUDA device the engine's calls fail and TSNE raises: nothing on the path
+    falls back to the CPU."""
+    import torch
+    from helpers import problem
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    X, G, P, _ = problem(300, seed=0, k=30, perplexity=10.0, dim=8, n_clusters=3)
+    with pytest.raises(RuntimeError):
+        TSNE(metric="precomputed", perplexity=10, max_iter=10, init="random").fit_transform(G)

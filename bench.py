@@ -12,12 +12,17 @@ init='random'. A step is one whole optimisation phase (tsne_run) on that input.
           tsne_init_with_P (upload of P and Y0, first H2 build), tsne_run, tsne_get_embedding,
           compute_kl_divergence, tsne_destroy
   roofline  the attractive pass fused with the update (the kernel launched every iteration)
-  cpu_baseline  the reference's own tsne_run (compiled from its sources in oracle/_ref) on a
-          bounded sample, all host cores; H2Pack's partition and bases, which are absent, are
-          the oracle's restatement behind the H2Pack interface (kind "reference"). Without
-          oracle/_ref, the oracle port (kind "port").
+  cpu_baseline  one whole run of the reference's own tsne_run (compiled from its sources in
+          oracle/_ref) on all host cores, on the same P and init, with the reference's own
+          per-stage profile; H2Pack's partition and bases, which are absent, are the oracle's
+          restatement behind the H2Pack interface (kind "reference"). Without oracle/_ref, a
+          bounded sample of the oracle port, extrapolated (kind "port").
+  parity_vs_reference  the final embeddings of that run and of the engine's last step scored
+          as the reference scores quality (benchmarks/quality.py): in-run KL, common-P KL,
+          10-NN and 30-NN preservation, with the pass criterion (KL within 1%, 30-NN within
+          0.5 points).
 
---impl reference times that same CPU path as its own line.
+--impl reference times whole runs of that same CPU path as its own line (steps = runs timed).
 Multi-GPU (torchrun): every rank runs its own replica of the workload (no collective on the
 data path); value is the slowest rank's time.
 """
@@ -74,6 +79,7 @@ def parse():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-runs", type=int, default=1, help="reference arm: whole runs timed")
     ap.add_argument("--save-embedding", default=None)
     ap.add_argument("--graph-cache", default=None, help="npz file holding the k-NN graph and P")
     ap.add_argument("--profile-csv", default=None, help="write the per-iteration stage CSV of the last step")
@@ -128,12 +134,12 @@ class Clocks:
 
     def __init__(self, index):
         self.index = index
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        import tempfile
+        self.path = Path(tempfile.gettempdir()) / f"tsne_bench_clocks_{os.getpid()}_{index}.csv"
         self.proc = None
 
     def start(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -163,6 +169,10 @@ class Clocks:
             for nm, v in zip(names, c[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
@@ -281,28 +291,25 @@ def ours(args, rank, world, local):
         if ck:
             out["clocks"] = ck
         if not args.no_cpu_baseline and world == 1:
-            out["cpu_baseline"] = cpu_sample(P, n, args.iters)
+            cb, Y_ref, kl_ref = cpu_sample(P, n, args.iters)
+            out["cpu_baseline"] = cb
+            if Y_ref is not None:
+                out["parity_vs_reference"] = parity(G, P, Yout, kl, Y_ref, kl_ref)
     return out
 
 
-def cpu_sample(P, n, iters):
-    """Bounded CPU sample of the same workload on all host cores: the reference's own loop
-    (oracle/_ref) when it was built, else the oracle port."""
-    try:
-        return _ref_sample(P, n, iters)
-    except Exception as e:   # the reference build is absent or failed: time the port
-        out = _port_sample(P, n, iters)
-        out["sample"] += f" (the reference's own loop was unavailable: {str(e)[:120]})"
-        return out
+PUBLISHED_SPLIT = {"attractive": 7.8, "h2_rebuild": 10.7, "h2_product": 8.5, "other": 0.9,
+                   "source": "reference benchmarks/results/REPORT.md:205 (Zheng 1M, 2D, 12 threads of an "
+                             "Apple M5 Max, H2Pack's own construction; not this hardware or data)"}
 
 
-def _ref_sample(P, n, iters):
-    """The reference's own tsne_run (its sources compiled in oracle/_ref: attractive pass,
-    rebuild schedule, fused H2 product, Z identity, update) with H2Pack's partition and
-    bases, which are absent, restated by the oracle behind the H2Pack interface. Iterations
-    0-2 with its stage profile; iterations 1 and 2 (each an H2 build + product + attractive
-    pass + update) give the per-stage times, and the phase estimate uses the schedule's
-    counts (rebuilds, passes; a force is reused between rebuilds)."""
+def ref_full_run(P, n, iters, warm=False):
+    """The reference's own tsne_run over the whole schedule (its sources compiled in
+    oracle/_ref: attractive pass, rebuild schedule, fused H2 product, Z identity, update,
+    renumbering, KL) on all host cores, on the benchmark's P and init. H2Pack's partition and
+    bases, which are absent, are the oracle's restatement behind the H2Pack interface. Times
+    tsne_run alone (the reference's "Total optimization time") and reads the reference's own
+    per-stage profile. warm: iterations 0-2 only (a warm-up)."""
     import tempfile
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
@@ -310,22 +317,94 @@ def _ref_sample(P, n, iters):
         raise RuntimeError("oracle/_ref is not built")
     cores = os.cpu_count() or 1
     Y0 = O.init_embedding(n, 2, 1)
+    tm = {}
     with tempfile.TemporaryDirectory() as td:
         f = Path(td) / "stages.csv"
-        t0 = time.perf_counter()
-        O.ref_run(P, Y0, 3, learning_rate=max(n / 12.0, 200.0), h2=True, nthreads=cores, attr_f32=2, profile=f)
-        wall = time.perf_counter() - t0
+        Y, kl = O.ref_run(P, Y0, 3 if warm else iters, learning_rate=max(n / 12.0, 200.0), h2=True,
+                          nthreads=cores, attr_f32=2, profile=f, timing=tm)
         st = O.ref_profile_csv(f)
-    t_rb = float(st["h2_rebuild"][1:3].mean())
-    t_prod = float((st["h2_matvec_s"] + st["h2_matvec_v"] + st["z_computation"])[1:3].mean())
-    t_pass = float((st["p_matvec"] + st["gradient"] + st["other"])[1:3].mean())
-    n_rb = rebuild_count(iters)
-    est = n_rb * (t_rb + t_prod) + iters * t_pass
-    return {"value": round(est, 2), "unit": "s", "cores": cores, "kind": "reference",
-            "sample": f"the reference's own tsne_run (built from its sources; H2Pack's partition and bases, absent, "
-                      f"restated by the oracle) on iterations 0-2 of the {n:,}-point workload ({wall:.1f} s with "
-                      f"setup); estimate = {n_rb} x (H2 build {t_rb:.3f} s + product {t_prod:.3f} s) + {iters} x "
-                      f"(attractive pass + update {t_pass:.4f} s)"}
+    split = {"attractive": float(st["p_matvec"].sum()), "h2_rebuild": float(st["h2_rebuild"].sum()),
+             "h2_product": float((st["h2_matvec_s"] + st["h2_matvec_v"] + st["z_computation"]).sum()),
+             "other": float((st["gradient"] + st["other"]).sum())}
+    return {"run_s": tm["run_s"], "split_s": {k: round(v, 2) for k, v in split.items()}, "kl": float(kl),
+            "Y": Y, "cores": cores}
+
+
+def ref_sample_text(n, iters):
+    return (f"one whole {iters}-iteration run of the reference's own tsne_run (built from its sources in "
+            f"oracle/_ref; H2Pack's partition and bases, absent, restated by the oracle) on the {n:,}-point "
+            f"workload's P and init, all host cores; timed: tsne_run alone")
+
+
+def cpu_sample(P, n, iters):
+    """CPU baseline on all host cores: a whole run of the reference's own loop (oracle/_ref)
+    when it was built, else a bounded sample of the oracle port (an estimate, labelled so).
+    Returns (cpu_baseline dict, reference embedding or None, reference KL or None)."""
+    try:
+        r = ref_full_run(P, n, iters)
+    except Exception as e:   # the reference build is absent or failed: time the port
+        out = _port_sample(P, n, iters)
+        out["sample"] += f" (the reference's own loop was unavailable: {str(e)[:120]})"
+        return out, None, None
+    out = {"value": round(r["run_s"], 2), "unit": "s", "cores": r["cores"], "kind": "reference",
+           "sample": ref_sample_text(n, iters), "split_s": r["split_s"], "kl_divergence": round(r["kl"], 5),
+           "published_split_s": PUBLISHED_SPLIT}
+    return out, r["Y"], r["kl"]
+
+
+def quality(G, P, Y, k_list=(10, 30), n_eval=5000, n_anchors=1000):
+    """The reference's quality scores (benchmarks/quality.py:56-90): k-NN preservation of
+    n_eval seeded query points (the input-space neighbours are the first k of the exact
+    graph, the embedding's from a KD-tree) and the common-P KL with Z estimated from
+    n_anchors seeded anchor rows. Y: (2, n)."""
+    from sklearn.neighbors import KDTree
+    n = P.shape[0]
+    Yp = np.ascontiguousarray(np.asarray(Y, dtype=np.float64).T)
+    rng = np.random.default_rng(0)
+    queries = rng.choice(n, size=min(n_eval, n), replace=False)
+    k_g = np.diff(G.indptr)
+    out = {}
+    tree = KDTree(Yp)
+    ld = tree.query(Yp[queries], k=max(k_list) + 1, return_distance=False)[:, 1:]
+    for k in k_list:
+        hits = 0
+        for r, i in enumerate(queries):
+            a, b = G.indptr[i], G.indptr[i + 1]
+            hd = G.indices[a:b][np.argsort(G.data[a:b], kind="stable")[:k]]
+            hits += len(set(hd.tolist()) & set(ld[r, :k].tolist()))
+        out[f"knn{k}"] = hits / (k * len(queries))
+    assert k_g.min() >= max(k_list)
+    rows = np.repeat(np.arange(n), np.diff(P.indptr))
+    d2 = np.zeros(P.nnz)
+    for c in range(Yp.shape[1]):
+        d2 += (Yp[rows, c] - Yp[P.indices, c]) ** 2
+    anchors = rng.choice(n, size=min(n_anchors, n), replace=False)
+    sums = np.empty(len(anchors))
+    for a, i in enumerate(anchors):
+        w = 1.0 / (1.0 + np.sum((Yp - Yp[i]) ** 2, axis=1))
+        w[i] = 0.0
+        sums[a] = w.sum()
+    Z = n * sums.mean()
+    p = P.data
+    out["kl_common_P"] = float(np.sum(p * np.log(np.maximum(p, 1e-300))) + np.sum(p * np.log1p(d2)) + np.log(Z))
+    return out
+
+
+def parity(G, P, Y_ours, kl_ours, Y_ref, kl_ref):
+    """Final-state parity of the engine's run with the reference loop's run on the same P and
+    init: in-run KL within 1%, common-P KL within 1%, 30-NN preservation within 0.5 points."""
+    qo, qr = quality(G, P, Y_ours), quality(G, P, Y_ref)
+    out = {"kl_run": {"ours": round(kl_ours, 5), "reference": round(kl_ref, 5),
+                      "rel_diff": round((kl_ours - kl_ref) / kl_ref, 5)},
+           "kl_common_P": {"ours": round(qo["kl_common_P"], 5), "reference": round(qr["kl_common_P"], 5),
+                           "rel_diff": round((qo["kl_common_P"] - qr["kl_common_P"]) / qr["kl_common_P"], 5)}}
+    for k in (10, 30):
+        out[f"knn{k}_preservation"] = {"ours": round(qo[f"knn{k}"], 4), "reference": round(qr[f"knn{k}"], 4),
+                                       "diff_points": round(100 * (qo[f"knn{k}"] - qr[f"knn{k}"]), 2)}
+    out["pass"] = bool(abs(out["kl_run"]["rel_diff"]) <= 0.01 and abs(out["kl_common_P"]["rel_diff"]) <= 0.01
+                       and abs(out["knn30_preservation"]["diff_points"]) <= 0.5)
+    out["criteria"] = "KL (in-run and common-P) within 1%, 30-NN preservation within 0.5 points of the reference run"
+    return out
 
 
 def _port_sample(P, n, iters):
@@ -528,16 +607,27 @@ def rebuild_count(iters, freq=3, early=10, exag_iter=250):
 
 
 def reference(args, rank, world, local):
+    """The reference arm: whole runs of the reference's own loop on the host cores. A step is
+    a whole 1000-iteration run (about a minute on 16 cores at 1M points), so the arm times
+    --ref-runs of them (default 1) after a warm-up of iterations 0-2, whatever --steps and
+    --warmup ask, and says so in the line."""
     if rank != 0:
         return None
     n = args.n
     X, G, P = workload(n, device=local, cache=args.graph_cache)
-    samples = [cpu_sample(P, n, args.iters) for _ in range(args.warmup + args.steps)][args.warmup:]
-    v = float(np.mean([s["value"] for s in samples]))
-    cb = dict(samples[-1])
-    cb["value"] = round(v, 2)
-    return {"impl": "reference", "metric": metric_name(n, args.iters), "value": round(v, 2), "unit": "s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v * 1e3, 1), "higher_is_better": False,
+    ref_full_run(P, n, args.iters, warm=True)
+    runs = [ref_full_run(P, n, args.iters) for _ in range(max(1, args.ref_runs))]
+    v = float(np.mean([r["run_s"] for r in runs]))
+    cb = {"value": round(v, 2), "unit": "s", "cores": runs[0]["cores"], "kind": "reference",
+          "sample": ref_sample_text(n, args.iters), "split_s": runs[-1]["split_s"],
+          "kl_divergence": round(runs[-1]["kl"], 5), "published_split_s": PUBLISHED_SPLIT}
+    return {"impl": "reference", "metric": metric_name(n, args.iters), "value": round(v, 2), "unit": "s",
+            "n_gpus": world, "steps": len(runs), "warmup": 1, "steps_requested": args.steps,
+            "warmup_requested": args.warmup,
+            "steps_note": "a step is one whole optimisation phase of the reference loop on the host cores; the arm "
+                          "times --ref-runs of them (default 1) after one warm-up of iterations 0-2, so that the "
+                          "command ends within a few minutes",
+            "ms_per_step": round(v * 1e3, 1), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": data_desc(n),
             "config": {"workload": f"{n:,} points x 50 dims -> 2D, {args.iters} iterations, perplexity 30, "

@@ -203,6 +203,14 @@ TSNE_API int tsne_h2_get_ranks(H2Pack_p h2, int *rank);
  * *max_rank are set. 0 on success, -1 without a built matrix. */
 TSNE_API int tsne_h2_get_bases(H2Pack_p h2, int *n_rows, int *max_rank, long long *row_off, float *U,
                                float *skel);
+/* Failure-path test of the dependency-ordered H2 launches (no counterpart in the reference):
+ * one device wait, bounded to max_polls polls (1 .. 2^22, about 0.1 us each), on a tree-node
+ * flag that nothing publishes. The wait gives up and records the failure in the matrix, as a
+ * real wait that ran out would; the next rebuild reports it, so the workspace's next
+ * tsne_run / tsne_run_range returns -1. Other workspaces are unaffected. Returns 1 when the
+ * failure was recorded, -1 without a built matrix, with max_polls out of range or on a CUDA
+ * error. */
+TSNE_API int tsne_h2_probe_dependency_timeout(H2Pack_p h2, int max_polls);
 /* Current device state in the caller's order: Y (low_dim x n_point), and the repulsive
  * force of the last rebuild (low_dim x n_point, NULL to skip) */
 TSNE_API int tsne_get_state(tsne_workspace_t *workspace, DTYPE *Y_out, DTYPE *rep_out, DTYPE *rep_Z);
@@ -224,8 +232,13 @@ TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, lon
  * device synchronisation of an allocation is not acceptable, or hosts with their own
  * allocator). Y (input) and F (output) are device arrays of n_point x low_dim floats,
  * point-major (x0, y0[, z0], x1, ...); Z is a device double receiving the normalisation.
- * F_i = (4 / Z) sum_{j != i} (1 + |y_i - y_j|^2)^-2 (y_i - y_j), Z from the identity of the
- * reference (src/tsne_h2pack.c:555-590) on the exact sums.
+ * F must not overlap Y (an overlapping call is rejected with -1).
+ * F_i = (4 / Z) sum_{j != i} (1 + |y_i - y_j|^2)^-2 (y_i - y_j) and
+ * Z = sum_{i != j} (1 + |y_i - y_j|^2)^-1: the reference's exact force and Z
+ * (src/tsne_h2pack.c:404-491), summed pair by pair instead of through its identity
+ * Z = sum s + 2 sum |y|^2 s - 2 sum y.v, which loses digits in single precision when the
+ * embedding is wide. If Z is not positive and finite (Y holds a NaN or an infinity), *Z
+ * receives it and F is set to zero: check *Z after the call when Y may be bad.
  *
  * The scratch lives in a file-scope __device__ array sized for at most 65536 points (about
  * 1 MB, held by every device that loads the library until the process exits); larger

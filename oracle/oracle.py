@@ -12,6 +12,7 @@ Two native libraries back it:
                         build time)
 """
 import ctypes
+import time
 import os
 from pathlib import Path
 
@@ -390,7 +391,7 @@ def ref_init_embedding(n, d, seed):
 
 def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=250,
             sklearn_compatible=1, nthreads=1, attr_f32=0, h2=False, h2_tol=1e-2, h2_rebuild_freq=3,
-            h2_rebuild_freq_early=10, h2_leaf_size=100, attr_generic=False, profile=None):
+            h2_rebuild_freq_early=10, h2_leaf_size=100, attr_generic=False, profile=None, timing=None):
     """The reference's own tsne_run; P: symmetric normalised scipy CSR; Y0: (d, n).
 
     h2=False: its exact-repulsion path (h2_rebuild_freq=999999, i.e. method='exact').
@@ -399,7 +400,9 @@ def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=
     renumbering, fused product, Z identity and force run on the oracle's matrices.
     attr_generic selects its FP64 attractive pass (TSNE_ATTR_GENERIC=1) instead of the
     2D single-precision gather. profile: a path; the reference writes its per-iteration
-    stage times there (tsne_write_profiling_data's CSV), read back by ref_profile_csv."""
+    stage times there (tsne_write_profiling_data's CSV), read back by ref_profile_csv.
+    timing: a dict that receives 'run_s', the wall time of tsne_run alone (the reference's
+    optimisation phase)."""
     L = ref_lib()
     os.environ["TSNE_ATTR_F32"] = str(attr_f32)
     os.environ["TSNE_ATTR_GENERIC"] = "1" if attr_generic else "0"
@@ -424,8 +427,11 @@ def ref_run(P, Y0, n_iter, learning_rate=None, early_exag=12.0, early_exag_iter=
     if not ws:
         raise RuntimeError("reference tsne_init_with_P returned NULL")
     try:
+        t0 = time.perf_counter()
         if L.tsne_run(ws) != 0:
             raise RuntimeError("reference tsne_run failed")
+        if timing is not None:
+            timing["run_s"] = time.perf_counter() - t0
         Y = np.zeros((d, n))
         L.tsne_get_embedding(ws, _p(Y, _f64p))
         kl_val = L.compute_kl_divergence(ws)

@@ -181,3 +181,21 @@ def _bind_inspection(lib):
                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
     lib.tsne_h2_matmul.restype = ctypes.c_int
     _bound.add(id(lib))
+
+
+def exact_Z_torch(Y, rows_per_block=512):
+    """Z = sum_{i != j} (1 + |y_i - y_j|^2)^-1 over all pairs, in FP64 on the GPU with torch (a
+    plain pairwise sum, independent of the engine; checked against the oracle's exact Z in
+    the tests). Y: (d, n)."""
+    import torch
+    Yt = torch.tensor(np.ascontiguousarray(np.asarray(Y, dtype=np.float64).T), device="cuda")
+    n = Yt.shape[0]
+    sq = (Yt * Yt).sum(1)
+    total = torch.zeros((), dtype=torch.float64, device="cuda")
+    for s in range(0, n, rows_per_block):
+        blk = Yt[s:s + rows_per_block]
+        r2 = torch.addmm(sq[None, :], blk, Yt.T, beta=1.0, alpha=-2.0)
+        r2 += sq[s:s + rows_per_block, None] + 1.0
+        total += r2.clamp_(min=1.0).reciprocal_().sum()
+        total -= blk.shape[0]          # the diagonal: r = 0 contributes 1 per row
+    return float(total.item())

@@ -34,3 +34,21 @@ def test_reference_arm_prints_one_contract_line(tmp_path):
     cb = out["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == out["value"]
     assert cb["sample"]
+    assert out["steps"] >= 1 and "steps_requested" in out and cb["split_s"]["h2_rebuild"] >= 0
+
+
+def test_parity_scores_on_the_cpu():
+    """bench.parity: an embedding against itself passes with zero differences; against a
+    scrambled copy it fails (the scores see the neighbourhoods)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    import oracle as O
+    n = 3000
+    X, G, P, _ = problem(n, seed=2, dim=20)
+    Y, kl = O.run(P.tocsr(), O.init_embedding(n, 2, 1), n_iter=300)
+    out = bench.parity(G.tocsr(), P.tocsr(), Y, kl, Y, kl)
+    assert out["pass"] and out["knn30_preservation"]["diff_points"] == 0 and out["kl_run"]["rel_diff"] == 0
+    assert out["knn10_preservation"]["ours"] > 0.1
+    Ys = Y[:, np.random.default_rng(0).permutation(n)]
+    bad = bench.parity(G.tocsr(), P.tocsr(), Ys, kl, Y, kl)
+    assert not bad["pass"] and bad["knn30_preservation"]["diff_points"] < -5

@@ -134,3 +134,29 @@ def test_coincident_points(mid):
     Y[:, idx] = Y[:, idx[:1]]
     biggest = _check_h2(P, Y, 100)
     assert biggest >= 150
+
+
+def test_dependency_wait_timeout_is_reported(mid):
+    """The failure path of the bounded waits in the dependency-ordered H2 launches: one wait,
+    limited to 1000 polls, on a node flag that nothing publishes gives up and records the
+    failure; the workspace's next run reports it (-1) instead of using the matrix, and a new
+    workspace in the same process still runs (the device context is intact)."""
+    X, G, P, _ = mid
+    Y0 = O.init_embedding(P.shape[0], 2, 4)
+    eng = Engine(P, Y0, n_iter=40)
+    lib = eng.lib
+    lib.tsne_h2_probe_dependency_timeout.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.tsne_h2_probe_dependency_timeout.restype = ctypes.c_int
+    eng.run(0, 5)
+    h = lib.tsne_get_h2_matrix(eng.ws)
+    assert h
+    assert lib.tsne_h2_probe_dependency_timeout(h, 0) == -1          # out of range: nothing launched
+    assert lib.tsne_h2_probe_dependency_timeout(h, 1000) == 1
+    with pytest.raises(RuntimeError):
+        eng.run(5, 10)
+    eng.close()
+    eng = Engine(P, Y0, n_iter=29)
+    eng.run_all()
+    _, klo = O.run(P, Y0, n_iter=29)
+    assert abs(eng.kl() - klo) < 5e-3 * abs(klo)
+    eng.close()

@@ -332,7 +332,7 @@ int rebuild_h2(tsne_workspace *ws, const std::function<void()> *overlap = nullpt
     const int rc = ws->h2->build(ws->Y.p, leaf, tol, overlap);
     ws->n_launch += ws->h2->launches() - l0;
     if (rc < 0) {
-        fprintf(stderr, "ERROR: Y contains NaN or Inf!\n");
+        if (rc == -1) fprintf(stderr, "ERROR: Y contains NaN or Inf!\n");
         ws->h2_valid = false;
         return -1;
     }
@@ -1227,6 +1227,12 @@ int tsne_h2_get_bases(H2Pack_p h2, int *n_rows, int *max_rank, long long *row_of
     if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2 || n_rows == nullptr || max_rank == nullptr) return -1;
     if (U != nullptr && (row_off == nullptr || skel == nullptr)) return -1;
     try { return h2->ws->h2->copy_bases(n_rows, max_rank, row_off, U, skel); } catch (const CudaError &) { return -1; }
+}
+
+int tsne_h2_probe_dependency_timeout(H2Pack_p h2, int max_polls)
+{
+    if (h2 == nullptr || h2->ws == nullptr || !h2->ws->h2 || max_polls < 1 || max_polls > (1 << 22)) return -1;
+    try { return h2->ws->h2->probe_dependency_timeout(max_polls); } catch (const CudaError &) { return -1; }
 }
 
 int tsne_get_state(tsne_workspace_t *ws, double *Y_out, double *rep_out, double *rep_Z)

@@ -440,6 +440,7 @@ struct DepArgs {
     int *ticket;    // work-item counter, zeroed before the launch
     int *err;       // set when a wait gave up
     int epoch;
+    int limit = DEP_WAIT_LIMIT;   // polls before a wait gives up
 };
 
 __device__ __forceinline__ int ld_acquire_gpu(const int *p)
@@ -456,7 +457,7 @@ __device__ __forceinline__ void st_release_gpu(int *p, int v)
 __device__ __forceinline__ void dep_wait(const DepArgs &dp, int node)
 {
     const int *f = dp.flag + node;
-    for (int it = 0; it < DEP_WAIT_LIMIT; it++) {
+    for (int it = 0; it < dp.limit; it++) {
         if (ld_acquire_gpu(f) == dp.epoch) return;
         __nanosleep(100);
     }
@@ -467,6 +468,12 @@ __device__ __forceinline__ void dep_publish(const DepArgs &dp, int node)
 {
     __threadfence();
     st_release_gpu(dp.flag + node, dp.epoch);
+}
+
+// one bounded wait for `node` (the failure path of the dependency-ordered launches, for tests)
+__global__ void k_dep_probe(DepArgs dp, int node)
+{
+    if (threadIdx.x == 0) dep_wait(dp, node);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1820,9 +1827,9 @@ public:
             TSNE_CUDA_CHECK(cudaEventSynchronize(counts_ev_));
             const TreeInfo &I = *hinfo_.p;
             if (I.nonfinite) return -1;
-            if (I.pad[1]) {   // a dependency wait of the previous build gave up
-                fprintf(stderr, "tsne_h2pack: H2 basis construction lost a dependency wait\n");
-                return -1;
+            if (I.pad[1]) {   // a dependency wait of an earlier launch gave up
+                fprintf(stderr, "tsne_h2pack: an H2 kernel gave up waiting for a tree dependency\n");
+                return -2;
             }
             if (I.pad[0]) {   // node table full: grow and start over
                 cap_node_ *= 2;
@@ -2095,6 +2102,16 @@ public:
     }
 
     long long launches() const override { return launches_; }
+
+    int probe_dependency_timeout(int polls) override
+    {
+        if (n_node_ <= 0) return -1;
+        // an epoch that no launch has published: the wait runs out after `polls` polls
+        DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], epoch_ + (1 << 24), polls};
+        k_dep_probe<<<1, 32, 0, st_>>>(dp, 0);
+        launches_++;
+        return wait_failed();
+    }
 
     int wait_failed() override
     {

@@ -21,7 +21,8 @@ class H2Matrix {
 public:
     virtual ~H2Matrix() = default;
     // Build for the points Y (device, point order). Returns 0 on success, -1 when Y holds
-    // a non-finite coordinate, 1 when the tree is too shallow for an H2 matrix
+    // a non-finite coordinate, -2 when a bounded dependency wait of an earlier launch gave
+    // up, 1 when the tree is too shallow for an H2 matrix
     // (max_level <= 2: the caller uses the exact sums). `overlap`, when given, is called
     // once, after the tree and list-count kernels are queued and before the host waits for
     // their counts: work it queues on the stream keeps the GPU busy meanwhile (it must not
@@ -50,6 +51,10 @@ public:
     // 1 when a bounded wait of a dependency-ordered launch gave up since the last build
     // (its results are not to be trusted); synchronises the stream
     virtual int wait_failed() = 0;
+    // Test of the failure path: one dependency wait, bounded to `polls` polls, on a node flag
+    // that nothing publishes. The wait gives up and records the failure that the next build
+    // reports. Returns wait_failed() (1), or -1 before any build.
+    virtual int probe_dependency_timeout(int polls) = 0;
     // prints and clears the per-phase device times gathered under TSNE_H2_TIMERS=1
     virtual void flush_timers() = 0;
 };

@@ -127,6 +127,37 @@ TSNE_API int tsne_fit_transform(const DTYPE *X, int n_point, int pt_dim, int low
 TSNE_API int tsne_fit_transform_with_P(const DTYPE *X, int n_point, int pt_dim, int low_dim,
                               const tsne_params_t *params, sparse_matrix_t *P, DTYPE *Y_out);
 
+/* ---- P built on the device (no counterpart entry point in the reference: these do the
+ * reference's calibration, src/tsne_utils.c:1022-1105, and the symmetrisation and
+ * normalisation its Python layer does on the host, tsne_h2pack/_backend.py:709-718) ---- */
+
+/* Symmetric normalised P = (P_c + P_c^T) / sum from a k-NN distance graph, P_c the
+ * conditional probabilities at `perplexity`: every step on the device. The graph's rows must
+ * be sorted by column, without self entries (as _backend.prepare_knn_graph leaves them);
+ * entries whose symmetric sum is exactly zero are dropped, as scipy's addition drops them.
+ * Entry values equal the reference's host computation bit for bit except for the total
+ * (a fixed-order device sum instead of numpy's). Returns a C-allocated matrix (free with
+ * sparse_matrix_destroy); NULL on bad input (reported on stderr) or a device error. */
+TSNE_API sparse_matrix_t *tsne_joint_P_from_knn_distances(const DTYPE *knn_distances, const int *knn_indices,
+                                                          const int *knn_indptr, int n_samples, int nnz,
+                                                          DTYPE perplexity);
+
+/* tsne_init_with_P with P built on the device from a k-NN distance graph, as
+ * tsne_joint_P_from_knn_distances does at params->perplexity: P never visits the host. The
+ * graph arrays are read during the call only. NULL on bad input or a device error. */
+TSNE_API tsne_workspace_t *tsne_init_with_knn_distances(const DTYPE *X, int n_point, int pt_dim, int low_dim,
+                                                        const tsne_params_t *params, const DTYPE *knn_distances,
+                                                        const int *knn_indices, const int *knn_indptr, int nnz);
+
+/* Exact k nearest neighbours (Euclidean) of every row of X (n_samples x n_features, row-major
+ * float32, host) on the device: the graph the reference's Python front ends build on the host
+ * (tsne_h2pack/_knn_methods.py:71-119, knn_method='exact'; no counterpart entry point in its C
+ * ABI). indices and distances (host, n_samples x k each) receive each row's k neighbours
+ * sorted by index, self excluded, distances not squared (single precision; ties of distance
+ * keep the smaller index). 1 <= k <= min(n_samples - 1, 256), n_samples <= 2^24. Returns 0,
+ * -1 on bad arguments, -2 on a device error. */
+TSNE_API int tsne_knn_graph(const float *X, int n_samples, int n_features, int k, int *indices, float *distances);
+
 /* ---- sparse matrix utilities (reference tsne_h2pack.h:269-295, src/tsne_utils.c:18-60) ---- */
 TSNE_API sparse_matrix_t *sparse_matrix_create(int n_rows, int n_cols, int nnz);
 TSNE_API void sparse_matrix_destroy(sparse_matrix_t *mat);

@@ -3,7 +3,8 @@ package (_backend.py's loader, ctypes signatures and marshalling, manifold.py's 
 this engine's libtsne_h2pack.so from its _lib/ directory and runs method='h2pack' and
 method='exact' on a precomputed graph. The results must equal, bit for bit, those of this
 repository's own package on the same input (the same library underneath, the same
-parameters mapped onto tsne_params_t, the same host-side P).
+parameters mapped onto tsne_params_t, the same host-side P: this package's own default builds
+P on the device instead, so the test selects its host path with TSNE_HOST_P=1).
 
 The reference package is staged by build() in baseline/_ref/tsne_h2pack (a copy of the
 reference checkout's package, as `pip install --target` would place it); the test copies it
@@ -34,7 +35,7 @@ CASES = [dict(method="h2pack", init="random", random_state=3, max_iter=300),
          dict(method="h2pack", init="pca", random_state=5, max_iter=120, n_components=3)]
 
 
-def test_reference_package_drives_this_library(tmp_path):
+def test_reference_package_drives_this_library(tmp_path, monkeypatch):
     pkg = tmp_path / "tsne_h2pack"
     shutil.copytree(REF_PKG, pkg)
     (pkg / "_lib").mkdir(exist_ok=True)
@@ -76,6 +77,7 @@ def test_reference_package_drives_this_library(tmp_path):
 
     from sklearn.decomposition import PCA
     from tsne_h2pack import TSNE
+    monkeypatch.setenv("TSNE_HOST_P", "1")     # P symmetrised on the host, as the reference package does
     for i, c in enumerate(CASES):
         c = dict(c)
         init = c.pop("init")

@@ -23,6 +23,7 @@
 #include "devbuf.h"
 #include "h2.h"
 #include "kernels.h"
+#include "pjoint.h"
 #include "../../include/tsne_h2pack.h"
 
 using namespace tsne;
@@ -49,7 +50,8 @@ __global__ void k_pad_len(int n, const int *__restrict__ rp, int *__restrict__ l
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         len[i] = (rp[i + 1] - rp[i] + 3) & ~3;
 }
-__global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restrict__ ci, const float *__restrict__ pv,
+template <typename V>
+__global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restrict__ ci, const V *__restrict__ pv,
                            const int *__restrict__ rpp, int *__restrict__ col, float *__restrict__ val)
 {
     const int lane = threadIdx.x & 31;
@@ -58,7 +60,7 @@ __global__ void k_pad_copy(int n, const int *__restrict__ rp, const int *__restr
         const int b = rp[i], len = rp[i + 1] - b, o = rpp[i], plen = rpp[i + 1] - o;
         for (int e = lane; e < plen; e += 32) {
             col[o + e] = e < len ? ci[b + e] : i;
-            val[o + e] = e < len ? pv[b + e] : 0.f;
+            val[o + e] = e < len ? (float)pv[b + e] : 0.f;
         }
     }
 }
@@ -219,6 +221,9 @@ bool csr_rows_valid(const sparse_matrix_t *P)
     return P->row_ptr[n] == 0 || (P->col_idx != nullptr && P->values != nullptr);
 }
 
+template <typename V>
+void pad_P(tsne_workspace *ws, const int *rp0, const int *ci0, const V *pv0);
+
 void upload_P(tsne_workspace *ws)
 {
     const int n = ws->n, nnz = ws->P->row_ptr[n];
@@ -264,9 +269,19 @@ void upload_P(tsne_workspace *ws)
     }
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     if (tm) printf("E2E upload_P: alloc + copies %.1f ms\n", 1e3 * (wall_sec() - t0));
+    pad_P(ws, rp0.p, ci0.p, pv0.p);
+}
+
+// The workspace's padded single-precision CSR from a device CSR (row pointers rp0, columns
+// ci0, values pv0 of type V)
+template <typename V>
+void pad_P(tsne_workspace *ws, const int *rp0, const int *ci0, const V *pv0)
+{
+    const int n = ws->n;
+    cudaStream_t st = ws->st;
     ws->len.exact(n + 1);
     ws->rp.exact(n + 2);
-    k_pad_len<<<ceil_div(n, 256), 256, 0, st>>>(n, rp0.p, ws->len.p);
+    k_pad_len<<<ceil_div(n, 256), 256, 0, st>>>(n, rp0, ws->len.p);
     TSNE_CUDA_CHECK(cudaMemsetAsync(ws->rp.p, 0, sizeof(int), st));
     size_t bytes = 0;
     TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(nullptr, bytes, ws->len.p, ws->rp.p + 1, n, st));
@@ -279,7 +294,7 @@ void upload_P(tsne_workspace *ws)
     ws->col.exact(std::max(padded, 4));
     ws->val.exact(std::max(padded, 4));
     ws->padded_nnz = padded;
-    k_pad_copy<<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, rp0.p, ci0.p, pv0.p, ws->rp.p, ws->col.p, ws->val.p);
+    k_pad_copy<V><<<ROW_GRID, ROW_BLOCK, 0, st>>>(n, rp0, ci0, pv0, ws->rp.p, ws->col.p, ws->val.p);
     TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     ws->n_launch += 3;
 }
@@ -826,25 +841,21 @@ sparse_matrix_t *compute_P_from_knn_distances(const double *knn_distances, const
     return P;
 }
 
-tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int low_dim,
-                                   const tsne_params_t *params, sparse_matrix_t *P)
+}  // extern "C"
+
+namespace {
+// Workspace creation once the arguments are checked: device state, P (through load_P, which
+// returns false on bad input), the initial embedding and the first H2 build. P (host, may be
+// NULL) is owned by the workspace from here on, as tsne_init_with_P specifies.
+tsne_workspace *create_workspace(int n_point, int pt_dim, int low_dim, const tsne_params_t *params,
+                                 sparse_matrix_t *P, const std::function<bool(tsne_workspace *)> &load_P)
 {
-    (void)X;
-    if (low_dim != 2 && low_dim != 3) {
-        printf("Error: low_dim must be 2 or 3 (got %d)\n", low_dim);
+    tsne_workspace *ws = nullptr;
+    try {
+        ws = new tsne_workspace();   // its pinned host scalars need a device
+    } catch (const CudaError &) {
         return nullptr;
     }
-    if (P == nullptr || P->n_rows != n_point || P->n_cols != n_point) {
-        printf("Error: Invalid P matrix (expected %dx%d, got %dx%d)\n", n_point, n_point, P ? P->n_rows : 0,
-               P ? P->n_cols : 0);
-        return nullptr;
-    }
-    if (params == nullptr || n_point < 1) return nullptr;
-    if (!csr_rows_valid(P)) {
-        printf("Error: Invalid P matrix (row pointers must start at 0 and not decrease)\n");
-        return nullptr;
-    }
-    tsne_workspace *ws = new tsne_workspace();
     try {
         ws->params = *params;
         if (params->profiling_output_file) ws->prof_file = params->profiling_output_file;
@@ -872,8 +883,11 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         ws->klpart.exact(ROW_GRID);
         const bool tm = env_int("TSNE_E2E_TIMERS", 0) != 0;
         double t0 = wall_sec();
-        upload_P(ws);
-        if (tm) printf("E2E init: upload_P %.1f ms\n", 1e3 * (wall_sec() - t0));
+        if (!load_P(ws)) {
+            tsne_destroy(ws);
+            return nullptr;
+        }
+        if (tm) printf("E2E init: P on the device %.1f ms\n", 1e3 * (wall_sec() - t0));
         t0 = wall_sec();
         std::vector<double> Y0((size_t)n_point * low_dim);
         initialize_embedding(Y0.data(), n_point, low_dim, params->init_method, params->init_Y,
@@ -919,6 +933,55 @@ tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int
         return nullptr;
     }
     return ws;
+}
+}  // namespace
+
+extern "C" {
+
+tsne_workspace_t *tsne_init_with_P(const double *X, int n_point, int pt_dim, int low_dim,
+                                   const tsne_params_t *params, sparse_matrix_t *P)
+{
+    (void)X;
+    if (low_dim != 2 && low_dim != 3) {
+        printf("Error: low_dim must be 2 or 3 (got %d)\n", low_dim);
+        return nullptr;
+    }
+    if (P == nullptr || P->n_rows != n_point || P->n_cols != n_point) {
+        printf("Error: Invalid P matrix (expected %dx%d, got %dx%d)\n", n_point, n_point, P ? P->n_rows : 0,
+               P ? P->n_cols : 0);
+        return nullptr;
+    }
+    if (params == nullptr || n_point < 1) return nullptr;
+    if (!csr_rows_valid(P)) {
+        printf("Error: Invalid P matrix (row pointers must start at 0 and not decrease)\n");
+        return nullptr;
+    }
+    return create_workspace(n_point, pt_dim, low_dim, params, P, [](tsne_workspace *w) {
+        upload_P(w);
+        return true;
+    });
+}
+
+tsne_workspace_t *tsne_init_with_knn_distances(const double *X, int n_point, int pt_dim, int low_dim,
+                                               const tsne_params_t *params, const double *knn_distances,
+                                               const int *knn_indices, const int *knn_indptr, int nnz)
+{
+    (void)X;
+    if (low_dim != 2 && low_dim != 3) {
+        printf("Error: low_dim must be 2 or 3 (got %d)\n", low_dim);
+        return nullptr;
+    }
+    if (params == nullptr || n_point < 1 || knn_indptr == nullptr || nnz < 0 ||
+        (nnz > 0 && (knn_distances == nullptr || knn_indices == nullptr)))
+        return nullptr;
+    const double perplexity = params->perplexity;
+    return create_workspace(n_point, pt_dim, low_dim, params, nullptr, [=](tsne_workspace *w) {
+        DevCSR d;
+        if (joint_P_device(w->st, n_point, knn_distances, knn_indices, knn_indptr, nnz, perplexity, d) != 0)
+            return false;
+        pad_P<double>(w, d.rp.p, d.col.p, d.val.p);
+        return true;
+    });
 }
 
 int tsne_run_range(tsne_workspace_t *ws, int iter_begin, int iter_end)

@@ -1,8 +1,10 @@
-// Legacy feature-space entry points of the C ABI: compute_sparse_P (reference
-// src/tsne_utils.c:828-933, there a ball-tree k-NN on the host), tsne_init and
-// tsne_fit_transform. Here the exact k nearest neighbours (k = 3 * perplexity) are found by a
-// brute-force device scan, the conditional P by the device beta bisection, and P is
-// symmetrised as P + P^T and normalised, as the reference's Python backend does
+// The k-NN graph on the device, and the feature-space entry points of the C ABI built on it:
+// tsne_knn_graph (the exact graph the reference's Python front ends compute on the host,
+// tsne_h2pack/_knn_methods.py:71-119), compute_sparse_P (reference src/tsne_utils.c:828-933,
+// there a ball-tree k-NN on the host), tsne_init and tsne_fit_transform. The exact k nearest
+// neighbours (k = 3 * perplexity for compute_sparse_P) come from a tiled device scan, the
+// conditional P from the device beta bisection, and P is symmetrised as P + P^T and normalised
+// on the device (pjoint.cu), as the reference's Python backend does on the host
 // (tsne_h2pack/_backend.py:709-718).
 #include <math.h>
 #include <stdlib.h>
@@ -16,21 +18,40 @@
 #include "common.cuh"
 #include "devbuf.h"
 #include "kernels.h"
+#include "pjoint.h"
 #include "../../include/tsne_h2pack.h"
 
 using namespace tsne;
 
 namespace {
 
-constexpr int KNN_MAX_K = 256;
+// ---------------------------------------------------------------------------------
+// Exact k nearest neighbours by a tiled scan. A CTA of 256 threads owns 64 query rows and
+// walks every point in tiles of 128, starting at its own tile and wrapping around (the
+// nearest points tend to lie near the query in the input order, so the per-row threshold
+// tightens early). Distances: d^2 = |q|^2 + |p|^2 - 2 q.p in FP32, the dot products
+// register-tiled (each thread 4 queries x 8 points, operands staged dimension-major in shared
+// memory). A distance below its row's threshold (the k-th best so far; +inf until k are known)
+// is appended to the row's candidate buffer in shared memory; after a tile, rows whose buffer
+// holds more than KBUF entries are merged by one warp (bitonic sort of the buffer by (d^2,
+// index), keep the first k, new threshold = the k-th). Ties keep the smaller index. The output
+// rows are sorted by index (as the calibration expects them), distances not squared.
+// ---------------------------------------------------------------------------------
+constexpr int KNN_MAX_K = 128;          // largest k of the tiled scan (perplexity <= 42)
+constexpr int KQ = 64;                  // queries per CTA
+constexpr int KT = 128;                 // points per tile
+constexpr int KBUF = 128;               // buffer slots that hold the current best k
+constexpr int KCAP = KBUF + KT;         // a row's buffer: best k + one tile of candidates
+constexpr int KNN_THREADS = 256;
+constexpr int KNN_WARP_MAX_K = 256;
 
-// One warp per query: distances to every point in chunks of 32, a sorted top-k list in
+// One warp per query (k above the tiled scan's limit, or more than 120 dimensions): distances to every point in chunks of 32, a sorted top-k list in
 // shared memory updated by warp-cooperative insertion. Ties keep the smaller index.
 __global__ void __launch_bounds__(128)
-k_knn(int n, int dim, const float *__restrict__ X, int k, int *__restrict__ out_idx, float *__restrict__ out_d2)
+k_knn_warp(int n, int dim, const float *__restrict__ X, int k, int *__restrict__ out_idx, float *__restrict__ out_d2)
 {
-    __shared__ float sd[4][KNN_MAX_K];
-    __shared__ int si[4][KNN_MAX_K];
+    __shared__ float sd[4][KNN_WARP_MAX_K];
+    __shared__ int si[4][KNN_WARP_MAX_K];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *bd = sd[w];
     int *bi = si[w];
@@ -77,96 +98,285 @@ k_knn(int n, int dim, const float *__restrict__ X, int k, int *__restrict__ out_
     }
 }
 
+
+size_t knn_smem_bytes(int dp)
+{
+    return sizeof(float) * ((size_t)dp * (KQ + KT) + KQ + KT + 2 * KQ) + sizeof(int) * 2 * KQ +
+           (sizeof(float) + sizeof(int)) * (size_t)KQ * KCAP;
+}
+
+// one warp sorts a row's buffer (KCAP = 256 entries, +inf / INT_MAX beyond `m`) ascending by
+// (key, tie) with a bitonic network
+__device__ void warp_bitonic(float *key, int *tie, int lane)
+{
+    for (int size = 2; size <= KCAP; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < KCAP / 2; t += 32) {
+                const int a = 2 * stride * (t / stride) + (t % stride), b = a + stride;
+                const bool up = (a & size) == 0;
+                const float ka = key[a], kb = key[b];
+                const int ia = tie[a], ib = tie[b];
+                const bool gt = ka > kb || (ka == kb && ia > ib);
+                if (gt == up) { key[a] = kb; key[b] = ka; tie[a] = ib; tie[b] = ia; }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(KNN_THREADS, 1)
+k_knn_tiled(int n, int dp, int k, const float *__restrict__ X, const float *__restrict__ xn,
+            int *__restrict__ out_idx, float *__restrict__ out_d)
+{
+    extern __shared__ float smem[];
+    float *qs = smem;                         // [dp][KQ]
+    float *ps = qs + (size_t)dp * KQ;         // [dp][KT]
+    float *qn = ps + (size_t)dp * KT;         // [KQ]
+    float *pn = qn + KQ;                      // [KT]
+    float *tau = pn + KT;                     // [KQ] threshold: the k-th best d^2 so far
+    int *taui = reinterpret_cast<int *>(tau + KQ);       // [KQ] its index (ties)
+    int *cnt = taui + KQ;                     // [KQ]
+    float *bd = reinterpret_cast<float *>(cnt + KQ);     // [KQ][KCAP]
+    int *bi = reinterpret_cast<int *>(bd + (size_t)KQ * KCAP);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int q0 = blockIdx.x * KQ;
+    const int dq = dp >> 2;
+    for (int idx = tid; idx < KQ * dq; idx += KNN_THREADS) {
+        const int q = idx % KQ, c4 = idx / KQ;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (q0 + q < n) v = *reinterpret_cast<const float4 *>(X + (size_t)(q0 + q) * dp + 4 * c4);
+        qs[(4 * c4 + 0) * KQ + q] = v.x;
+        qs[(4 * c4 + 1) * KQ + q] = v.y;
+        qs[(4 * c4 + 2) * KQ + q] = v.z;
+        qs[(4 * c4 + 3) * KQ + q] = v.w;
+    }
+    if (tid < KQ) {
+        qn[tid] = q0 + tid < n ? xn[q0 + tid] : 0.f;
+        tau[tid] = INFINITY;
+        taui[tid] = INT_MAX;
+        cnt[tid] = 0;
+    }
+    for (int idx = tid; idx < KQ * KCAP; idx += KNN_THREADS) { bd[idx] = INFINITY; bi[idx] = INT_MAX; }
+    const int ty = tid >> 4, tx = tid & 15;   // queries ty*4 .. +3; points tx*4 .. +3 and 64 + tx*4 .. +3
+    const int ntile = (n + KT - 1) / KT;
+    const int t0 = q0 / KT;
+    for (int tt = 0; tt < ntile; tt++) {
+        const int p0 = ((t0 + tt) % ntile) * KT;
+        __syncthreads();
+        for (int idx = tid; idx < KT * dq; idx += KNN_THREADS) {
+            const int p = idx % KT, c4 = idx / KT;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (p0 + p < n) v = *reinterpret_cast<const float4 *>(X + (size_t)(p0 + p) * dp + 4 * c4);
+            ps[(4 * c4 + 0) * KT + p] = v.x;
+            ps[(4 * c4 + 1) * KT + p] = v.y;
+            ps[(4 * c4 + 2) * KT + p] = v.z;
+            ps[(4 * c4 + 3) * KT + p] = v.w;
+        }
+        if (tid < KT) pn[tid] = p0 + tid < n ? xn[p0 + tid] : 0.f;
+        __syncthreads();
+        float acc[4][8];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+#pragma unroll 4
+        for (int c = 0; c < dp; c++) {
+            const float4 a = *reinterpret_cast<const float4 *>(qs + c * KQ + ty * 4);
+            const float4 b0 = *reinterpret_cast<const float4 *>(ps + c * KT + tx * 4);
+            const float4 b1 = *reinterpret_cast<const float4 *>(ps + c * KT + 64 + tx * 4);
+            const float av[4] = {a.x, a.y, a.z, a.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = ty * 4 + i, qi = q0 + r;
+            if (qi >= n) continue;
+            const float th = tau[r];
+            const int thi = taui[r];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int p = (j < 4 ? 0 : 64) + tx * 4 + (j & 3);
+                const int gi = p0 + p;
+                if (gi >= n || gi == qi) continue;
+                const float d = fmaxf(fmaf(-2.f, acc[i][j], qn[r] + pn[p]), 0.f);
+                if (d < th || (d == th && gi < thi)) {
+                    const int slot = atomicAdd(&cnt[r], 1);
+                    bd[(size_t)r * KCAP + slot] = d;
+                    bi[(size_t)r * KCAP + slot] = gi;
+                }
+            }
+        }
+        __syncthreads();
+        const bool last = tt == ntile - 1;
+        for (int r = wid; r < KQ; r += KNN_THREADS / 32) {
+            const int m = cnt[r];
+            if (!(m > KBUF || (last && m > 0))) continue;
+            warp_bitonic(bd + (size_t)r * KCAP, bi + (size_t)r * KCAP, lane);
+            const int keep = min(m, k);
+            for (int t = keep + lane; t < KCAP; t += 32) { bd[(size_t)r * KCAP + t] = INFINITY; bi[(size_t)r * KCAP + t] = INT_MAX; }
+            if (lane == 0) {
+                cnt[r] = keep;
+                if (keep == k) { tau[r] = bd[(size_t)r * KCAP + k - 1]; taui[r] = bi[(size_t)r * KCAP + k - 1]; }
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // rows re-sorted by index for the output
+    for (int r = wid; r < KQ; r += KNN_THREADS / 32) {
+        const int qi = q0 + r;
+        if (qi >= n) continue;
+        float *key = bd + (size_t)r * KCAP;
+        int *tie = bi + (size_t)r * KCAP;
+        for (int t = lane; t < KCAP; t += 32) {
+            // sort by index: the index becomes the key (exactly representable below 2^24), the
+            // squared distance rides along in the tie slot as its bits
+            const int ix = tie[t];
+            const float dv = key[t];
+            const bool used = t < k;
+            key[t] = used ? (float)ix : INFINITY;
+            tie[t] = used ? __float_as_int(dv) : INT_MAX;
+        }
+        __syncwarp();
+        warp_bitonic(key, tie, lane);
+        for (int t = lane; t < k; t += 32) {
+            out_idx[(size_t)qi * k + t] = (int)key[t];
+            out_d[(size_t)qi * k + t] = sqrtf(__int_as_float(tie[t]));
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
+namespace tsne {
+
+// k-NN graph of the n x dim float rows of X (host, row-major) on the device: indices and
+// distances (n x k each, host), rows sorted by index. 0 ok, -1 bad arguments.
+int knn_graph_device(const float *X, int n, int dim, int k, int *idx_out, float *dist_out)
+{
+    if (X == nullptr || n < 2 || dim < 1 || k < 1 || k > n - 1 || k > KNN_WARP_MAX_K || n > (1 << 24)) return -1;
+    const int dp = (dim + 3) & ~3;
+    const size_t smem = knn_smem_bytes(dp);
+    const bool tiled = k <= KNN_MAX_K && smem <= 227 * 1024;
+    cudaStream_t st;
+    TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    {
+        AllocStream guard(st);
+        // centred (distances unchanged; the norms, and so the cancellation in
+        // |q|^2 + |p|^2 - 2 q.p, shrink)
+        std::vector<double> mean(dim, 0.0);
+        for (int i = 0; i < n; i++)
+            for (int c = 0; c < dim; c++) mean[c] += X[(size_t)i * dim + c];
+        for (int c = 0; c < dim; c++) mean[c] /= n;
+        std::vector<float> Xp((size_t)n * dp, 0.f), nrm(n);
+        for (int i = 0; i < n; i++) {
+            float s2 = 0.f;
+            for (int c = 0; c < dim; c++) {
+                const float v = (float)((double)X[(size_t)i * dim + c] - mean[c]);
+                Xp[(size_t)i * dp + c] = v;
+                s2 = fmaf(v, v, s2);
+            }
+            nrm[i] = s2;
+        }
+        DevBuf<float> dX, dN, dD;
+        DevBuf<int> dI;
+        dX.exact(Xp.size()); dN.exact(n); dD.exact((size_t)n * k); dI.exact((size_t)n * k);
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(dX.p, Xp.data(), sizeof(float) * Xp.size(), cudaMemcpyHostToDevice, st));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(dN.p, nrm.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+        if (tiled) {
+            TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_knn_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_knn_tiled<<<(n + KQ - 1) / KQ, KNN_THREADS, smem, st>>>(n, dp, k, dX.p, dN.p, dI.p, dD.p);
+        } else {
+            // squared distances sorted by (distance, index); re-sorted by index on the host below
+            k_knn_warp<<<std::min((n + 3) / 4, 148 * 32), 128, 0, st>>>(n, dp, dX.p, k, dI.p, dD.p);
+        }
+        TSNE_CUDA_CHECK(cudaGetLastError());
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(idx_out, dI.p, sizeof(int) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+        TSNE_CUDA_CHECK(cudaMemcpyAsync(dist_out, dD.p, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    cudaStreamDestroy(st);
+    if (!tiled) {
+        std::vector<std::pair<int, float>> row(k);
+        for (int i = 0; i < n; i++) {
+            for (int j = 0; j < k; j++) row[j] = {idx_out[(size_t)i * k + j], dist_out[(size_t)i * k + j]};
+            std::sort(row.begin(), row.end());
+            for (int j = 0; j < k; j++) {
+                idx_out[(size_t)i * k + j] = row[j].first;
+                dist_out[(size_t)i * k + j] = sqrtf(row[j].second);
+            }
+        }
+    }
+    return 0;
+}
+
+}  // namespace tsne
+
 extern "C" {
+
+int tsne_knn_graph(const float *X, int n_samples, int n_features, int k, int *indices, float *distances)
+{
+    if (indices == nullptr || distances == nullptr) return -1;
+    try {
+        return knn_graph_device(X, n_samples, n_features, k, indices, distances);
+    } catch (const CudaError &) {
+        return -2;
+    }
+}
 
 sparse_matrix_t *compute_sparse_P(const double *X, int n_point, int pt_dim, double perplexity, int use_vptree,
                                   int verbose, int num_threads)
 {
     (void)use_vptree;
+    (void)num_threads;
     if (X == nullptr || n_point < 2 || pt_dim < 1 || perplexity <= 0.0) return nullptr;
     int k = (int)(3.0 * perplexity);
     if (k > n_point - 1) k = n_point - 1;
-    if (k < 1 || k > KNN_MAX_K) {
-        fprintf(stderr, "Error: k = %d neighbours is outside [1, %d]\n", k, KNN_MAX_K);
+    if (k < 1 || k > KNN_WARP_MAX_K) {
+        fprintf(stderr, "Error: k = %d neighbours is outside [1, %d]\n", k, KNN_WARP_MAX_K);
         return nullptr;
     }
-    if (verbose) printf("Computing %d nearest neighbours on the device (brute force)...\n", k);
+    if (verbose) printf("Computing %d nearest neighbours on the device (exact, tiled scan)...\n", k);
     std::vector<float> Xr((size_t)n_point * pt_dim);
     for (int i = 0; i < n_point; i++)
         for (int c = 0; c < pt_dim; c++) Xr[(size_t)i * pt_dim + c] = (float)X[(size_t)c * n_point + i];
-    std::vector<int> idx((size_t)n_point * k);
-    std::vector<float> d2((size_t)n_point * k);
+    std::vector<int> idx((size_t)n_point * k), indptr((size_t)n_point + 1);
+    std::vector<float> df((size_t)n_point * k);
     try {
+        if (knn_graph_device(Xr.data(), n_point, pt_dim, k, idx.data(), df.data()) != 0) return nullptr;
+        std::vector<double> dist(df.begin(), df.end());
+        for (int i = 0; i <= n_point; i++) indptr[i] = i * k;
         cudaStream_t st;
         TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        DevBuf<float> dX, dD;
-        DevBuf<int> dI;
-        dX.exact(Xr.size()); dD.exact(d2.size()); dI.exact(idx.size());
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(dX.p, Xr.data(), sizeof(float) * Xr.size(), cudaMemcpyHostToDevice, st));
-        k_knn<<<std::min(ceil_div(n_point, 4), 148 * 32), 128, 0, st>>>(n_point, pt_dim, dX.p, k, dI.p, dD.p);
-        TSNE_CUDA_CHECK(cudaGetLastError());
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(idx.data(), dI.p, sizeof(int) * idx.size(), cudaMemcpyDeviceToHost, st));
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(d2.data(), dD.p, sizeof(float) * d2.size(), cudaMemcpyDeviceToHost, st));
-        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+        sparse_matrix_t *P = nullptr;
+        {
+            AllocStream guard(st);
+            DevCSR d;
+            if (joint_P_device(st, n_point, dist.data(), idx.data(), indptr.data(), (long long)n_point * k,
+                               perplexity, d) == 0) {
+                P = sparse_matrix_create(n_point, n_point, (int)d.nnz);
+                if (P != nullptr) {
+                    TSNE_CUDA_CHECK(cudaMemcpyAsync(P->row_ptr, d.rp.p, sizeof(int) * ((size_t)n_point + 1),
+                                                    cudaMemcpyDeviceToHost, st));
+                    if (d.nnz > 0) {
+                        TSNE_CUDA_CHECK(cudaMemcpyAsync(P->col_idx, d.col.p, sizeof(int) * d.nnz, cudaMemcpyDeviceToHost, st));
+                        TSNE_CUDA_CHECK(cudaMemcpyAsync(P->values, d.val.p, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost, st));
+                    }
+                    TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+                    P->nnz = (int)d.nnz;
+                }
+            }
+        }
         cudaStreamDestroy(st);
+        return P;
     } catch (const CudaError &) {
         return nullptr;
     }
-    // rows sorted by column, as the reference backend hands them to the calibration
-    std::vector<int> indptr(n_point + 1), ind((size_t)n_point * k);
-    std::vector<double> dist((size_t)n_point * k);
-    std::vector<std::pair<int, float>> row(k);
-    for (int i = 0; i < n_point; i++) {
-        for (int j = 0; j < k; j++) row[j] = {idx[(size_t)i * k + j], d2[(size_t)i * k + j]};
-        std::sort(row.begin(), row.end());
-        for (int j = 0; j < k; j++) {
-            ind[(size_t)i * k + j] = row[j].first;
-            dist[(size_t)i * k + j] = sqrt((double)row[j].second);
-        }
-        indptr[i] = i * k;
-    }
-    indptr[n_point] = n_point * k;
-    sparse_matrix_t *Pc = compute_P_from_knn_distances(dist.data(), ind.data(), indptr.data(), n_point, n_point * k,
-                                                       perplexity, num_threads);
-    if (Pc == nullptr) return nullptr;
-    // P = (Pc + Pc^T) / sum
-    std::vector<int> cnt(n_point + 1, 0);
-    for (int i = 0; i < n_point; i++)
-        for (int e = Pc->row_ptr[i]; e < Pc->row_ptr[i + 1]; e++) { cnt[i]++; cnt[Pc->col_idx[e]]++; }
-    std::vector<int> start(n_point + 1, 0);
-    for (int i = 0; i < n_point; i++) start[i + 1] = start[i] + cnt[i];
-    std::vector<std::pair<int, double>> ent(start[n_point]);
-    std::vector<int> fill(start.begin(), start.end() - 1);
-    for (int i = 0; i < n_point; i++)
-        for (int e = Pc->row_ptr[i]; e < Pc->row_ptr[i + 1]; e++) {
-            const int j = Pc->col_idx[e];
-            ent[fill[i]++] = {j, Pc->values[e]};
-            ent[fill[j]++] = {i, Pc->values[e]};
-        }
-    sparse_matrix_destroy(Pc);
-    std::vector<int> rp(n_point + 1, 0), ci;
-    std::vector<double> pv;
-    ci.reserve(ent.size());
-    pv.reserve(ent.size());
-    double total = 0.0;
-    for (int i = 0; i < n_point; i++) {
-        std::sort(ent.begin() + start[i], ent.begin() + start[i + 1],
-                  [](const std::pair<int, double> &a, const std::pair<int, double> &b) { return a.first < b.first; });
-        for (int e = start[i]; e < start[i + 1]; e++) {
-            if (!ci.empty() && (int)ci.size() > rp[i] && ci.back() == ent[e].first) pv.back() += ent[e].second;
-            else { ci.push_back(ent[e].first); pv.push_back(ent[e].second); }
-        }
-        rp[i + 1] = (int)ci.size();
-    }
-    for (double x : pv) total += x;
-    sparse_matrix_t *P = sparse_matrix_create(n_point, n_point, (int)ci.size());
-    if (P == nullptr) return nullptr;
-    memcpy(P->row_ptr, rp.data(), sizeof(int) * (n_point + 1));
-    memcpy(P->col_idx, ci.data(), sizeof(int) * ci.size());
-    for (size_t e = 0; e < pv.size(); e++) P->values[e] = total > 0 ? pv[e] / total : pv[e];
-    return P;
 }
 
 tsne_workspace_t *tsne_init(const double *X, int n_point, int pt_dim, int low_dim, const tsne_params_t *params)

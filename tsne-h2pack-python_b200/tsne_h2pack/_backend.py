@@ -171,6 +171,16 @@ class TSNEBackend:
         lib.tsne_set_embedding.restype = ctypes.c_int
         lib.tsne_get_run_stats.argtypes = [ws_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]
         lib.tsne_get_run_stats.restype = ctypes.c_int
+        # P built on the device
+        lib.tsne_joint_P_from_knn_distances.argtypes = [
+            ctypes.POINTER(DTYPE), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+            ctypes.c_int, ctypes.c_double]
+        lib.tsne_joint_P_from_knn_distances.restype = ctypes.POINTER(SparseMatrix)
+        lib.tsne_init_with_knn_distances.argtypes = [
+            _optional_ndpointer(dtype=NP_DTYPE, flags="C_CONTIGUOUS", ndim=2), ctypes.c_int, ctypes.c_int,
+            ctypes.c_int, ctypes.POINTER(TSNEParams), ctypes.POINTER(DTYPE), ctypes.POINTER(ctypes.c_int),
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.tsne_init_with_knn_distances.restype = ws_p
 
     def create_default_params(self) -> TSNEParams:
         """Defaults of tsne_create_default_params, filled on the Python side (the reference
@@ -271,8 +281,36 @@ class TSNEBackend:
                 shape=knn_distances_csr.shape)
         return knn_distances_csr
 
+    @staticmethod
+    def _graph_arrays(G):
+        data = np.ascontiguousarray(G.data, dtype=NP_DTYPE)
+        ind = np.ascontiguousarray(G.indices, dtype=np.int32)
+        ptr = np.ascontiguousarray(G.indptr, dtype=np.int32)
+        return data, ind, ptr
+
+    def joint_P_device(self, knn_distances_csr, perplexity: float):
+        """The same P as joint_P with every step on the device (tsne_joint_P_from_knn_distances):
+        entries equal joint_P's bit for bit except for the normalising total's rounding."""
+        from scipy.sparse import csr_matrix
+        G = self.prepare_knn_graph(knn_distances_csr)
+        n = G.shape[0]
+        data, ind, ptr = self._graph_arrays(G)
+        m = self._lib.tsne_joint_P_from_knn_distances(
+            data.ctypes.data_as(ctypes.POINTER(DTYPE)), ind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            ptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, int(G.nnz), ctypes.c_double(perplexity))
+        if not m:
+            raise RuntimeError("tsne_joint_P_from_knn_distances returned NULL")
+        mc = m.contents
+        P = csr_matrix((np.ctypeslib.as_array(mc.values, shape=(mc.nnz,)).copy() if mc.nnz else np.zeros(0),
+                        np.ctypeslib.as_array(mc.col_idx, shape=(mc.nnz,)).copy() if mc.nnz else
+                        np.zeros(0, np.int32),
+                        np.ctypeslib.as_array(mc.row_ptr, shape=(mc.n_rows + 1,)).copy()), shape=(n, n))
+        self._lib.sparse_matrix_destroy(m)
+        return P
+
     def joint_P(self, knn_distances_csr, perplexity: float, num_threads: int = 1):
-        """Symmetric normalised P = (P_c + P_c^T) / sum from a k-NN distance graph."""
+        """Symmetric normalised P = (P_c + P_c^T) / sum from a k-NN distance graph (calibration
+        on the device, symmetrisation on the host, as the reference's _backend.py:672-718)."""
         G = self.prepare_knn_graph(knn_distances_csr)
         Pc = self.conditional_P(G, perplexity, num_threads)
         Ps = Pc + Pc.T
@@ -285,15 +323,23 @@ class TSNEBackend:
                                          params: TSNEParams, init_Y: Optional[np.ndarray] = None
                                          ) -> Tuple[np.ndarray, dict]:
         """Embed from a k-NN distance graph of any source (reference _backend.py:611-781):
-        calibrate P on the device, symmetrise, then init -> run -> embedding -> KL -> destroy."""
+        P calibrated, symmetrised and normalised on the device (tsne_init_with_knn_distances:
+        P never visits the host), then run -> embedding -> KL -> destroy. With the environment
+        switch TSNE_HOST_P=1, P is symmetrised on the host as the reference does
+        (tsne_init_with_P), which reproduces the reference package's results bit for bit."""
         from scipy.sparse import csr_matrix
         if not isinstance(knn_distances_csr, csr_matrix):
             raise TypeError(f"knn_distances must be scipy CSR matrix, got {type(knn_distances_csr)}")
         n = knn_distances_csr.shape[0]
         n_features = X.shape[1] if X is not None else 0
         t0 = time.time()
-        P = self.joint_P(knn_distances_csr, params.perplexity, params.num_threads)
-        P_c = scipy_csr_to_c_sparse_matrix(P, self._lib)
+        host_P = os.environ.get("TSNE_HOST_P", "0") not in ("", "0")
+        if host_P:
+            P = self.joint_P(knn_distances_csr, params.perplexity, params.num_threads)
+            P_c = scipy_csr_to_c_sparse_matrix(P, self._lib)
+        else:
+            G = self.prepare_knn_graph(knn_distances_csr)
+            gdata, gind, gptr = self._graph_arrays(G)
         p_time = time.time() - t0
         knn_time = getattr(knn_distances_csr, "knn_time", 0.0)
         Yc = np.zeros((n_components, n), dtype=NP_DTYPE)
@@ -308,7 +354,14 @@ class TSNEBackend:
         else:
             params.init_method = 0
             params.init_Y = None
-        ws = self._lib.tsne_init_with_P(None, n, n_features, n_components, ctypes.byref(params), P_c)
+        if host_P:
+            ws = self._lib.tsne_init_with_P(None, n, n_features, n_components, ctypes.byref(params), P_c)
+        else:
+            ws = self._lib.tsne_init_with_knn_distances(
+                None, n, n_features, n_components, ctypes.byref(params),
+                gdata.ctypes.data_as(ctypes.POINTER(DTYPE)), gind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                gptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(G.nnz))
+            p_time = time.time() - t0
         params.init_Y = None
         del init_c
         if not ws:

@@ -2,8 +2,9 @@
 matrix of L2 distances (self excluded), the contract of the reference's _knn_methods.py.
 
 The graph is built once per fit, outside the optimisation phase this package accelerates;
-'exact' and 'balltree' use scikit-learn, 'pynndescent' / 'faiss' / 'annoy' use those
-libraries when they are installed. Below 10K samples 'pynndescent' switches to the exact
+'exact' and 'balltree' use scikit-learn, 'cuda' the engine's exact device scan
+(tsne_knn_graph), 'pynndescent' / 'faiss' / 'annoy' use those libraries when they are
+installed. Below 10K samples 'pynndescent' switches to the exact
 graph, as the reference does.
 """
 import time
@@ -29,6 +30,31 @@ class ExactKNN(_KNN):
         from sklearn.neighbors import NearestNeighbors
         nn = NearestNeighbors(n_neighbors=k, algorithm="brute", n_jobs=n_jobs, **params).fit(X)
         return nn.kneighbors_graph(mode="distance")
+
+
+class CudaKNN(_KNN):
+    """The exact graph on the device (tsne_knn_graph: tiled FP32 scan, rows sorted by index);
+    the same neighbours as 'exact' except where two distances tie to single precision."""
+    name = "cuda"
+
+    def _graph(self, X, k, n_jobs, verbose, **params):
+        import ctypes
+        from scipy.sparse import csr_matrix
+        from ._backend import get_backend
+        lib = get_backend()._lib
+        Xf = np.ascontiguousarray(X, dtype=np.float32)
+        n, f = Xf.shape
+        idx = np.zeros((n, k), dtype=np.int32)
+        dist = np.zeros((n, k), dtype=np.float32)
+        lib.tsne_knn_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p]
+        lib.tsne_knn_graph.restype = ctypes.c_int
+        rc = lib.tsne_knn_graph(Xf.ctypes.data, n, f, k, idx.ctypes.data, dist.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"tsne_knn_graph failed ({rc}): k must be in [1, min(n - 1, 256)] and a CUDA "
+                               "device present")
+        return csr_matrix((dist.astype(np.float64).ravel(), idx.ravel(), np.arange(0, (n + 1) * k, k)),
+                          shape=(n, n))
 
 
 class BallTreeKNN(_KNN):
@@ -85,7 +111,7 @@ class AnnoyKNN(_KNN):
         raise NotImplementedError("knn_method='annoy' is not available in this package; use 'exact'")
 
 
-_METHODS = {c.name: c for c in (ExactKNN, BallTreeKNN, PyNNDescentKNN, FAISSKNN, AnnoyKNN)}
+_METHODS = {c.name: c for c in (ExactKNN, CudaKNN, BallTreeKNN, PyNNDescentKNN, FAISSKNN, AnnoyKNN)}
 
 
 def list_knn_methods():

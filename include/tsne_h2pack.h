@@ -158,6 +158,27 @@ TSNE_API tsne_workspace_t *tsne_init_with_knn_distances(const DTYPE *X, int n_po
  * -1 on bad arguments, -2 on a device error. */
 TSNE_API int tsne_knn_graph(const float *X, int n_samples, int n_features, int k, int *indices, float *distances);
 
+/* init='pca' on the device (reference tsne_h2pack/manifold.py:399-416, there scikit-learn's
+ * randomized PCA on the host; no counterpart entry point in its C ABI). X: n_samples x
+ * n_features, row-major FP64 (host). Y_out (host, n_samples x n_components, row-major) receives
+ * the exact principal-component projection of the centred data (each component's
+ * largest-magnitude loading positive, scikit-learn's sign rule) scaled to a first-coordinate
+ * standard deviation of 1e-4. 0 on success; -1 bad arguments (n_components above
+ * min(n_samples, n_features), n_features > 4096); -2 device error; -3 non-finite data or no
+ * variance along the first component. */
+TSNE_API int tsne_pca_init(const DTYPE *X, int n_samples, int n_features, int n_components, DTYPE *Y_out);
+
+/* Quality scores of an embedding (reference benchmarks/quality.py:56-90; no counterpart in its
+ * C ABI), on the device. Y: low_dim x n_point (the layout of tsne_get_embedding); P: a fixed
+ * joint P (host CSR). kl receives sum p log p + sum p log(1 + d^2) + log Z with Z the exact sum
+ * of (1 + d^2)^-1 over all ordered pairs (the reference estimates Z from anchor rows).
+ * knn_preservation receives the mean fraction of each query's k input-space neighbours
+ * (hd_neighbors, n_eval x k, row per query) found among its k nearest points in the embedding.
+ * 1 <= k <= 128. 0 on success, -1 bad arguments, -2 device error. */
+TSNE_API int tsne_score_embedding(const DTYPE *Y, int n_point, int low_dim, const sparse_matrix_t *P,
+                                  const int *queries, int n_eval, const int *hd_neighbors, int k,
+                                  DTYPE *knn_preservation, DTYPE *kl);
+
 /* ---- sparse matrix utilities (reference tsne_h2pack.h:269-295, src/tsne_utils.c:18-60) ---- */
 TSNE_API sparse_matrix_t *sparse_matrix_create(int n_rows, int n_cols, int nnz);
 TSNE_API void sparse_matrix_destroy(sparse_matrix_t *mat);

@@ -242,6 +242,56 @@ class TSNEBackend:
             raise RuntimeError(f"tsne_fit_transform_with_P failed with code {rc}")
         return np.ascontiguousarray(Yc.T), {"kl_divergence": 0.0, "n_iter": params.n_iter}
 
+    def pca_init(self, X: np.ndarray, n_components: int) -> np.ndarray:
+        """init='pca' on the device (tsne_pca_init): the exact PCA projection of X, scaled to a
+        first-coordinate standard deviation of 1e-4 (reference manifold.py:399-416, which uses
+        scikit-learn's randomized approximation of the same projection)."""
+        X = np.ascontiguousarray(X, dtype=NP_DTYPE)
+        n, f = X.shape
+        Y = np.zeros((n, n_components), dtype=NP_DTYPE)
+        self._lib.tsne_pca_init.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p]
+        self._lib.tsne_pca_init.restype = ctypes.c_int
+        rc = self._lib.tsne_pca_init(X.ctypes.data, n, f, int(n_components), Y.ctypes.data)
+        if rc == -3:
+            raise ValueError("init='pca' failed: X holds inf/NaN or has no variance along its first principal "
+                             "component; pass init='random'")
+        if rc != 0:
+            raise RuntimeError(f"tsne_pca_init failed ({rc})")
+        return Y
+
+    def score_embedding(self, Y: np.ndarray, P, knn_graph, k: int = 10, n_eval: int = 5000, seed: int = 0) -> dict:
+        """The reference's quality scores (benchmarks/quality.py:56-90) on the device
+        (tsne_score_embedding): k-NN preservation of n_eval seeded queries (input-space
+        neighbours: the k nearest of each row of knn_graph) and the KL divergence under P with
+        the exact Z. Y: (n_samples, n_components)."""
+        n, d = Y.shape
+        Yc = np.ascontiguousarray(np.asarray(Y, dtype=NP_DTYPE).T)
+        rng = np.random.default_rng(seed)
+        q = np.ascontiguousarray(rng.choice(n, size=min(n_eval, n), replace=False), dtype=np.int32)
+        G = knn_graph.tocsr()
+        hd = np.empty((len(q), k), dtype=np.int32)
+        for r, i in enumerate(q):
+            a, b = G.indptr[i], G.indptr[i + 1]
+            if b - a < k:
+                raise ValueError(f"row {i} of the k-NN graph has fewer than k = {k} neighbours")
+            hd[r] = G.indices[a:b][np.argsort(G.data[a:b], kind="stable")[:k]]
+        Pc = scipy_csr_to_c_sparse_matrix(P.tocsr(), self._lib)
+        kp, kl = ctypes.c_double(), ctypes.c_double()
+        self._lib.tsne_score_embedding.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.POINTER(SparseMatrix), ctypes.c_void_p, ctypes.c_int,
+                                                   ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                   ctypes.POINTER(ctypes.c_double)]
+        self._lib.tsne_score_embedding.restype = ctypes.c_int
+        try:
+            rc = self._lib.tsne_score_embedding(Yc.ctypes.data, n, d, Pc, q.ctypes.data, len(q), hd.ctypes.data, k,
+                                                ctypes.byref(kp), ctypes.byref(kl))
+        finally:
+            self._lib.sparse_matrix_destroy(Pc)
+        if rc != 0:
+            raise RuntimeError(f"tsne_score_embedding failed ({rc})")
+        return {"kl": kl.value, "knn_preservation": kp.value}
+
     def conditional_P(self, knn_distances_csr, perplexity: float, num_threads: int = 1):
         """P_j|i of a k-NN distance graph (CSR, L2 distances, rows sorted, no self entries)."""
         from scipy.sparse import csr_matrix

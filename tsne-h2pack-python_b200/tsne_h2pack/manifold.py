@@ -158,8 +158,9 @@ class TSNE:
 
     def _initial_embedding(self, X, n_samples: int) -> Optional[np.ndarray]:
         """(n_samples, n_components) initial Y, or None for 'random' (drawn by the engine from
-        random_state). 'pca' follows scikit-learn: randomized PCA scaled to a first-coordinate
-        standard deviation of 1e-4."""
+        random_state). 'pca' is the exact PCA projection computed on the device, scaled to a
+        first-coordinate standard deviation of 1e-4 (the reference uses scikit-learn's randomized
+        approximation of the same projection)."""
         self._validate_params()
         if isinstance(self.init, str):
             if self.init == "random":
@@ -173,17 +174,7 @@ class TSNE:
             if self.n_components > min(n_samples, n_features):
                 raise ValueError(f"init='pca' needs n_components={self.n_components} <= "
                                  f"min(n_samples, n_features)={min(n_samples, n_features)}")
-            from sklearn.decomposition import PCA
-            pca = PCA(n_components=self.n_components, svd_solver="randomized", random_state=self.random_state)
-            with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
-                Y = pca.fit_transform(np.asarray(X, dtype=np.float64))
-            if not np.isfinite(Y).all():
-                raise ValueError("init='pca' failed: the PCA of X is not finite; check X for inf/NaN or "
-                                 "pass init='random'")
-            std = np.std(Y[:, 0])
-            if not np.isfinite(std) or std == 0:
-                raise ValueError("init='pca' failed: X has no variance along its first principal component")
-            return Y / std * 1e-4
+            return get_backend().pca_init(np.asarray(X, dtype=np.float64), self.n_components)
         Y = np.array(self.init, dtype=np.float64)
         if Y.shape != (n_samples, self.n_components):
             raise ValueError(f"init array has shape {Y.shape}, expected (n_samples, n_components)="

@@ -302,6 +302,13 @@ TSNE_API int tsne_get_run_stats(tsne_workspace_t *workspace, int *n_rebuild, lon
 TSNE_API int tsne_exact_repulsion_static(const float *Y, int n_point, int low_dim, float *F, double *Z,
                                          void *stream);
 
+/* Measured compute ceilings of the current device (no counterpart in the reference), for the
+ * roofline of the non-tensor kernels: FP32 FMA throughput of scalar FFMA and of the paired
+ * fma.rn.f32x2 form (TFLOP/s, 2 flops per FMA and lane), and MUFU reciprocals (10^12 per
+ * second). Each is the best of five timed launches of a register-resident loop over every SM.
+ * 0 on success, -2 on a CUDA error. */
+TSNE_API int tsne_measure_compute_peaks(double *ffma_tflops, double *ffma2_tflops, double *rcp_tops);
+
 /* Device memory: workspaces take their buffers from the current device's stream-ordered
  * memory pool, which keeps freed memory for the next workspace (no counterpart in the
  * reference, which allocates on the host). This returns the pool's unused memory to the

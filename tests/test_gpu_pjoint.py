@@ -39,7 +39,7 @@ def _compare(G, perp):
     np.testing.assert_allclose(Pd.data, Ph.data, rtol=1e-12, atol=0)
     # the same sums before normalisation: the ratio of the two matrices is one number
     ratio = Pd.data / Ph.data
-    assert np.ptp(ratio) <= 4e-16 * ratio.mean()
+    assert np.ptp(ratio) <= 2e-15 * ratio.mean()
     return Ph, Pd
 
 

@@ -35,7 +35,8 @@ namespace {
 // is appended to the row's candidate buffer in shared memory; after a tile, rows whose buffer
 // holds more than KBUF entries are merged by one warp (bitonic sort of the buffer by (d^2,
 // index), keep the first k, new threshold = the k-th). Ties keep the smaller index. The output
-// rows are sorted by index (as the calibration expects them), distances not squared.
+// rows are sorted by index (as the calibration expects them); the reported distances (not
+// squared) are recomputed from the coordinates' differences.
 // ---------------------------------------------------------------------------------
 constexpr int KNN_MAX_K = 128;          // largest k of the tiled scan (perplexity <= 42)
 constexpr int KQ = 64;                  // queries per CTA
@@ -243,9 +244,20 @@ k_knn_tiled(int n, int dp, int k, const float *__restrict__ X, const float *__re
         }
         __syncwarp();
         warp_bitonic(key, tie, lane);
+        // the reported distances by direct differences (the selection's |q|^2 + |p|^2 - 2 q.p
+        // is exact enough to rank, not to report)
         for (int t = lane; t < k; t += 32) {
-            out_idx[(size_t)qi * k + t] = (int)key[t];
-            out_d[(size_t)qi * k + t] = sqrtf(__int_as_float(tie[t]));
+            const int j = (int)key[t];
+            const float *xq = X + (size_t)qi * dp, *xj = X + (size_t)j * dp;
+            float d2 = 0.f;
+            for (int c = 0; c < dp; c += 4) {
+                const float4 a4 = *reinterpret_cast<const float4 *>(xq + c);
+                const float4 b4 = *reinterpret_cast<const float4 *>(xj + c);
+                const float dx = a4.x - b4.x, dy = a4.y - b4.y, dz = a4.z - b4.z, dw = a4.w - b4.w;
+                d2 = fmaf(dx, dx, d2); d2 = fmaf(dy, dy, d2); d2 = fmaf(dz, dz, d2); d2 = fmaf(dw, dw, d2);
+            }
+            out_idx[(size_t)qi * k + t] = j;
+            out_d[(size_t)qi * k + t] = sqrtf(d2);
         }
         __syncwarp();
     }

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_force(int n, int nblk, const 
     const double c = ok ? 4.0 / Z : 0.0;
     const int i = blockIdx.x * NA_THREADS + threadIdx.x;
     if (i < n) {
-        const float4 gi = g[i];
+        const float4 gi = ok ? g[i] : make_float4(0.f, 0.f, 0.f, 0.f);   // 0 * NaN would be NaN
         F[(size_t)i * D + 0] = (float)(c * gi.x);
         F[(size_t)i * D + 1] = (float)(c * gi.y);
         if (D == 3) F[(size_t)i * D + D - 1] = (float)(c * gi.z);

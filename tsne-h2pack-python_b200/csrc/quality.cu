@@ -317,6 +317,7 @@ int tsne_pca_init(const double *X, int n_samples, int n_features, int n_componen
     const int npair = f * (f + 1) / 2;
     const int ny = (npair + PCA_THREADS * PCA_PAIRS - 1) / (PCA_THREADS * PCA_PAIRS);
     std::vector<double> gram_h(npair), Y((size_t)n * c);
+    bool finite = true;
     try {
         cudaStream_t st;
         TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -342,12 +343,9 @@ int tsne_pca_init(const double *X, int n_samples, int n_features, int n_componen
             std::vector<double> A((size_t)f * f), w, Vf;
             for (int a = 0, p = 0; a < f; a++)
                 for (int b = a; b < f; b++, p++) A[(size_t)a * f + b] = A[(size_t)b * f + a] = gram_h[p];
-            for (double x : A)
-                if (!std::isfinite(x)) {
-                    fprintf(stderr, "tsne_pca_init: the data hold a NaN or an infinity\n");
-                    cudaStreamDestroy(st);
-                    return -3;
-                }
+            for (double x : A) finite = finite && std::isfinite(x);
+            // (the stream outlives every buffer of this scope: they are freed on it)
+            if (finite) {
             jacobi_eigen(f, A, w, Vf);
             std::vector<int> ord(f);
             for (int i = 0; i < f; i++) ord[i] = i;
@@ -366,9 +364,15 @@ int tsne_pca_init(const double *X, int n_samples, int n_features, int n_componen
             k_project<<<148 * 8, 256, 0, st>>>(n, f, c, dX.p, mean.p, V.p, dY.p);
             TSNE_CUDA_CHECK(cudaGetLastError());
             TSNE_CUDA_CHECK(cudaMemcpyAsync(Y.data(), dY.p, sizeof(double) * Y.size(), cudaMemcpyDeviceToHost, st));
+            }
             TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
         }
+        TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
         cudaStreamDestroy(st);
+        if (!finite) {
+            fprintf(stderr, "tsne_pca_init: the data hold a NaN or an infinity\n");
+            return -3;
+        }
     } catch (const CudaError &) {
         return -2;
     }

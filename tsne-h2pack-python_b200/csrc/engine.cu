@@ -23,6 +23,7 @@
 #include "devbuf.h"
 #include "h2.h"
 #include "kernels.h"
+#include "attr_tiles.h"
 #include "pjoint.h"
 #include "../../include/tsne_h2pack.h"
 
@@ -136,6 +137,7 @@ struct tsne_workspace {
     HostPinned<DevScalars> hsc;
     DevBuf<double> part, zpart, klpart, convpart;
     DevBuf<unsigned char> cub_tmp;
+    AttrTiles tiles;                // 2D attractive pass over shared-column row tiles
     std::unique_ptr<H2Matrix> h2;
     bool h2_valid = false;
     bool has_order = false;
@@ -403,6 +405,7 @@ void renumber_impl(tsne_workspace *ws, const int *ord_dev)
     launch_permute_int(st, n, ord_dev, ws->has_order ? ws->order.p : nullptr, ws->order2.p, ws->has_order ? 0 : 1);
     ws->order.swap(ws->order2);
     ws->has_order = true;
+    ws->tiles.valid = false;        // rows changed: the tile format is rebuilt by the caller
     ws->n_launch += 11;
 }
 
@@ -422,6 +425,14 @@ void exact_force(tsne_workspace *ws)
     launch_exact_sv<D>(ws->st, ws->n, ws->Y.p, ws->s.p, ws->v.p);
     launch_z_force<D>(ws->st, ws->n, ws->Y.p, ws->s.p, ws->v.p, nullptr, ws->frc.p, ws->sc.p, ws->zpart.p, 0, 0);
     ws->n_launch += 3;
+}
+
+// the shared-memory window forms (TSNE_ATTR_WINDOW) are off: the CSR kernels that the tile
+// form pairs with (the update after a rebuild, the centring) use the ROW_GRID row split
+bool window_off()
+{
+    const char *e = getenv("TSNE_ATTR_WINDOW");
+    return e == nullptr || atoi(e) == 0;
 }
 
 bool next_reorder_due(tsne_workspace *ws, int iter, const int *iters, int n_reorder)
@@ -458,6 +469,10 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
             if (*c == ',') c++;
         }
     }
+    // the shared-column tile form of the 2D attractive pass, built at the renumberings from
+    // iteration tiles_from on (TSNE_ATTR_TILES=0 keeps the CSR pass throughout)
+    const bool tiles_on = env_int("TSNE_ATTR_TILES", 1) != 0 && window_off();
+    const int tiles_from = env_int("TSNE_ATTR_TILES_FROM", 100);
     const int h2_freq = p.h2_rebuild_freq > 0 ? p.h2_rebuild_freq : 10;
     const bool never_h2 = h2_freq > 100000;
     cudaStream_t st = ws->st;
@@ -503,13 +518,20 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
                 while (ws->next_reorder < n_reorder && iter >= reorder_iters[ws->next_reorder]) ws->next_reorder++;
                 const double t0 = wall_sec();
                 renumber(ws, ws->h2->perm_device());
+                if (D == 2 && tiles_on && iter >= tiles_from) {
+                    attr_tiles_build(st, n, ws->padded_nnz, ws->rp.p, ws->col.p, ws->tiles);
+                    ws->n_launch += 8;
+                }
                 if (env_int("TSNE_H2_TIMERS", 0)) printf("RENUMBER iter %d %.1f ms\n", iter, 1e3 * (wall_sec() - t0));
             }
             // the attractive sums of this iteration depend on Y only: they run while the host
             // waits for the build's counts
             const std::function<void()> overlap = [&]() {
                 ws->attr.exact(ws->vbytes * n);
-                launch_attr_grad<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->attr.p);
+                if (D == 2 && ws->tiles.valid)
+                    launch_attr_tile_grad(st, n, ws->tiles, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->attr.p);
+                else
+                    launch_attr_grad<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->attr.p);
                 attr_ready = true;
                 ws->n_launch++;
             };
@@ -569,8 +591,14 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
                              (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
         } else {
             if (ktime) stage_event(ws, kev, kused);
-            launch_attr_update<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p, ws->uY.p, ws->gains.p,
-                                  force, flag, (float)(4.0 * exag), (float)mom, (float)lr, ws->part.p);
+            if (D == 2 && ws->tiles.valid)
+                launch_attr_tile_update(st, n, ws->tiles, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p,
+                                        ws->uY.p, ws->gains.p, force, flag, (float)(4.0 * exag), (float)mom,
+                                        (float)lr, ws->part.p);
+            else
+                launch_attr_update<D>(st, n, ws->rp.p, ws->col.p, ws->val.p, ws->Y.p, ws->Yn.p, ws->uY.p,
+                                      ws->gains.p, force, flag, (float)(4.0 * exag), (float)mom, (float)lr,
+                                      ws->part.p);
             if (ktime) stage_event(ws, kev, kused);
         }
         if (prof) { stage_event(ws, evpool, evused); stages.push_back({iter, 0, e2, evused - 1}); }

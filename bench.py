@@ -228,6 +228,27 @@ def ours(args, rank, world, local):
                  "destroy": w5 - w4}
         return wall, run_ms.value / 1e3, attr_ms.value, attr_n.value, nl.value, nr.value, kl, parts
 
+    def stage_split():
+        """The engine's own per-stage device times of one more run (its profiling CSV, the
+        reference's schema): attractive pass + update, H2 rebuild, H2 product + force, other."""
+        import tempfile
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+        with tempfile.TemporaryDirectory() as td:
+            f = Path(td) / "stages.csv"
+            prm = params_for(be, n, args.iters)
+            prm.enable_profiling = 1
+            prm.profiling_output_file = str(f).encode()
+            ws = lib.tsne_init_with_P(None, n, 0, 2, ctypes.byref(prm), scipy_csr_to_c_sparse_matrix(P, lib))
+            if not ws or lib.tsne_run(ws) != 0:
+                raise RuntimeError("profiled run failed")
+            lib.tsne_destroy(ws)
+            st = O.ref_profile_csv(f)
+        return {"attractive": round(float(st["p_matvec"].sum()), 3),
+                "h2_rebuild": round(float(st["h2_rebuild"].sum()), 3),
+                "h2_product": round(float((st["h2_matvec_s"] + st["h2_matvec_v"] + st["z_computation"]).sum()), 3),
+                "other": round(float((st["gradient"] + st["other"]).sum()), 3)}
+
     for _ in range(args.warmup):
         step()
     dist = world > 1
@@ -288,6 +309,7 @@ def ours(args, rank, world, local):
             "kl_divergence": round(kl, 5),
             "n_rebuild": res[-1][5],
             "setup_s": round(setup_s, 1),
+            "split_s": stage_split() if world == 1 else None,
         }
         if ck:
             out["clocks"] = ck

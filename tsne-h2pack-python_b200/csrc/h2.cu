@@ -295,47 +295,70 @@ __global__ void __launch_bounds__(TREE_BLOCK) k_tree_marks(TreeView tv)
 }
 
 // one CTA: block offsets per level (exclusive scans over the blocks), level table, totals
-__global__ void __launch_bounds__(1024) k_tree_scan(int nblk, TreeView tv)
+// Exclusive scans of the 64 per-block count columns (a CTA per column; each thread takes a
+// contiguous run of blocks, then a block-wide scan of the runs). Column totals: the node
+// counts per level (columns 0-31) into btot[32 + l], the boundary counts |B_l| (columns 32-63)
+// into btot[l]; k_tree_levels turns the level counts into the node table's level ranges.
+constexpr int TREE_SCAN_THREADS = 1024;
+
+__global__ void __launch_bounds__(TREE_SCAN_THREADS) k_tree_scan(int nblk, TreeView tv)
 {
-    __shared__ int tot[2][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int col = w; col < 64; col += 32) {
-        int run = 0;
-        for (int b0 = 0; b0 < nblk; b0 += 32) {
-            const int b = b0 + lane;
-            const size_t at = ((size_t)b * 2 + (col >> 5)) * 32 + (col & 31);
-            const int v = b < nblk ? tv.blkcnt[at] : 0;
-            int x = v;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (b < nblk) tv.blkoff[at] = run + x - v;
-            run += __shfl_sync(0xffffffffu, x, 31);
+    __shared__ int wsum[TREE_SCAN_THREADS / 32];
+    const int col = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int per = (nblk + TREE_SCAN_THREADS - 1) / TREE_SCAN_THREADS;
+    const int b0 = min(nblk, tid * per), b1 = min(nblk, b0 + per);
+    auto at = [&](int b) { return ((size_t)b * 2 + (col >> 5)) * 32 + (col & 31); };
+    int own = 0;
+    for (int b = b0; b < b1; b++) own += tv.blkcnt[at(b)];
+    int x = own;   // inclusive scan of the runs: warps, then the warp totals
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
         }
-        if (lane == 0) tot[col >> 5][col & 31] = run;
+        wsum[lane] = t;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        TreeInfo *info = tv.info;
-        int acc = 0, maxl = 0;
-        for (int l = 0; l < 32; l++) {
-            const int c = l <= tv.L ? tot[0][l] : 0;
-            info->level_begin[l] = acc;
-            info->n_level_nodes[l] = c;
-            if (c > 0) maxl = l;
-            acc += c;
-            tv.btot[l] = l <= tv.L ? tot[1][l] : 0;
-        }
-        info->level_begin[32] = acc;
-        info->n_node = acc;
-        info->max_level = maxl;
-        if (acc > tv.cap_node) {   // node table full: the host regrows it; nothing downstream runs
-            info->pad[0] = 1;
-            info->n_node = 0;
-            info->max_level = 0;
-            for (int l = 0; l < 32; l++) info->n_level_nodes[l] = 0;
-        }
+    int run = x - own + (w > 0 ? wsum[w - 1] : 0);
+    for (int b = b0; b < b1; b++) {
+        const int v = tv.blkcnt[at(b)];
+        tv.blkoff[at(b)] = run;
+        run += v;
+    }
+    if (tid == TREE_SCAN_THREADS - 1) {
+        const int total = wsum[31];
+        if (col < 32) tv.btot[32 + col] = total;
+        else tv.btot[col - 32] = (col - 32) <= tv.L ? total : 0;
+    }
+}
+
+__global__ void k_tree_levels(TreeView tv)
+{
+    if (threadIdx.x != 0) return;
+    TreeInfo *info = tv.info;
+    int acc = 0, maxl = 0;
+    for (int l = 0; l < 32; l++) {
+        const int c = l <= tv.L ? tv.btot[32 + l] : 0;
+        info->level_begin[l] = acc;
+        info->n_level_nodes[l] = c;
+        if (c > 0) maxl = l;
+        acc += c;
+    }
+    info->level_begin[32] = acc;
+    info->n_node = acc;
+    info->max_level = maxl;
+    if (acc > tv.cap_node) {   // node table full: the host regrows it; nothing downstream runs
+        info->pad[0] = 1;
+        info->n_node = 0;
+        info->max_level = 0;
+        for (int l = 0; l < 32; l++) info->n_level_nodes[l] = 0;
     }
 }
 
@@ -1793,7 +1816,7 @@ public:
         fm_.exact(n);
         blkcnt_.exact((size_t)ceil_div(n, TREE_BLOCK) * 64);
         blkoff_.exact((size_t)ceil_div(n, TREE_BLOCK) * 64);
-        btot_.exact(32);
+        btot_.exact(64);
         ticket_.exact(1);
         info_.exact(1);
         TSNE_CUDA_CHECK(cudaMemsetAsync(info_.p, 0, sizeof(TreeInfo), st_));
@@ -1844,10 +1867,11 @@ public:
                 k_gather<D><<<grid_for(n_ + 1, 256), 256, 0, st_>>>(n_, L, perm_.p, (const Vec<D> *)Y,
                                                                      (Vec<D> *)xt_.p, keys_.p, delta_.p);
                 k_tree_marks<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());
-                k_tree_scan<<<1, 1024, 0, st_>>>(nblk, view());
+                k_tree_scan<<<64, TREE_SCAN_THREADS, 0, st_>>>(nblk, view());
+                k_tree_levels<<<1, 32, 0, st_>>>(view());
                 k_tree_emit<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());
                 k_tree_finish<D><<<grid_for(cap_node_, 256, 148 * 8), 256, 0, st_>>>(view());
-                launches_ += 9 + 4;
+                launches_ += 10 + 4;
                 tree_ok = true;
             }
             launch_list_counts();

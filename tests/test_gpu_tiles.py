@@ -6,7 +6,7 @@ it replaces after the renumberings:
     mean's FP64 summation order differs), and its KL after 200 iterations within 1e-3;
   - the same on a ragged P: isolated points, a 3000-entry hub row and a tile with more
     distinct columns than the shared-memory stage holds (read from global memory);
-  - n not a multiple of the 64-row tile.
+  - n not a multiple of the tile (64 and 32 rows).
 """
 import numpy as np
 import pytest
@@ -41,9 +41,10 @@ def _wide_tile(P, seed=1):
     return Q
 
 
-def _run(P, Y0, iters, tiles, monkeypatch):
+def _run(P, Y0, iters, tiles, monkeypatch, kind_rows=64):
     monkeypatch.setenv("TSNE_ATTR_TILES", "1" if tiles else "0")
     monkeypatch.setenv("TSNE_ATTR_TILES_FROM", "30")
+    monkeypatch.setenv("TSNE_ATTR_TILE_ROWS", "32" if kind_rows == 32 else "64")
     eng = Engine(P, Y0, n_iter=200)
     eng.run(0, iters)
     Y = eng.embedding() if iters < 200 else None
@@ -55,17 +56,17 @@ def _run(P, Y0, iters, tiles, monkeypatch):
     return Y, kl
 
 
-@pytest.mark.parametrize("kind", ["plain", "ragged"])
-def test_tiles_equal_csr_pass(mid, kind, monkeypatch):
+@pytest.mark.parametrize("kind,rows", [("plain", 64), ("ragged", 64), ("plain", 32)])
+def test_tiles_equal_csr_pass(mid, kind, rows, monkeypatch):
     X, G, P, _ = mid
     if kind == "ragged":
         from test_gpu_edges import _ragged
         P = _wide_tile(_ragged(P))
     Y0 = O.init_embedding(P.shape[0], 2, 3)
-    Ya, _ = _run(P, Y0, 32, False, monkeypatch)
-    Yb, _ = _run(P, Y0, 32, True, monkeypatch)
+    Ya, _ = _run(P, Y0, 32, False, monkeypatch, rows)
+    Yb, _ = _run(P, Y0, 32, True, monkeypatch, rows)
     assert rel(Yb, Ya) <= 1e-6
-    Ya, kla = _run(P, Y0, 200, False, monkeypatch)
-    Yb, klb = _run(P, Y0, 200, True, monkeypatch)
+    Ya, kla = _run(P, Y0, 200, False, monkeypatch, rows)
+    Yb, klb = _run(P, Y0, 200, True, monkeypatch, rows)
     print(f"{kind}: KL csr {kla:.6f} tiles {klb:.6f}")
     assert abs(klb - kla) <= 1e-3 * abs(kla)

@@ -10,9 +10,10 @@
 // read Y from there through 16-bit tile-local indices stored beside the values.
 //
 // Format (built on the device after each renumbering, rows unchanged): for tile t (rows
-// 64 t .. 64 t + 63) the sorted distinct columns ucol[uptr[t] .. uptr[t + 1]); for every
-// padded P entry its index into its tile's list (lidx, uint16). Tiles with more than
-// TILE_UMAX distinct columns (too many for the shared-memory stage) read Y[col] directly.
+// R t .. R t + R - 1) the sorted distinct columns ucol[uptr[t] .. uptr[t + 1]); for every
+// padded P entry its index into its tile's list (lidx, uint16). Tiles with more than umax
+// distinct columns (too many for the shared-memory stage) read Y[col] directly. The stage is
+// filled with asynchronous 8-byte copies (cp.async), all of a thread's gathers in flight at once.
 //
 // The kernel keeps k_attr_update's arithmetic exactly: a row per half-warp, lane l of the half
 // summing entries b + 4 l + 64 s in the same order, the same 16-lane reduction and the same
@@ -21,6 +22,8 @@
 // so the mean is a fixed-order sum, though in another order than the CSR pass's.
 #include <cuda_runtime.h>
 #include <stdio.h>
+
+#include <algorithm>
 
 #include <cub/cub.cuh>
 
@@ -32,14 +35,23 @@ namespace tsne {
 
 namespace {
 
-constexpr int TILE_R = 64;                  // rows per tile
-constexpr int TILE_THREADS = 256;           // 16 half-warps: four rows each per tile
-constexpr int TILE_GRID = 148 * 4;          // persistent CTAs (four per SM)
-constexpr int TILE_UMAX = 6144;             // distinct columns staged per tile (48 KB)
-constexpr size_t TILE_SMEM = sizeof(float2) * TILE_UMAX;
+constexpr int TILE_THREADS = 256;           // 16 half-warps, rows / 16 rows each per tile
+constexpr int TILE_GRID = 148 * 4;          // persistent CTAs: at most four per SM (registers)
+constexpr int TILE_UMAX_CAP = 12288;        // largest shared-memory stage (96 KB)
 static_assert(TILE_GRID <= ROW_GRID, "the centring reads ROW_GRID partial slots");
 
 enum { T_FUSED = 0, T_GRAD = 1 };
+
+// 8-byte asynchronous copy global -> shared (the gathers of a tile's stage all in flight)
+__device__ __forceinline__ void cp_async8(float2 *dst, const float2 *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
 
 __device__ __forceinline__ void acc_pair(const float2 &yi, const float2 &yj, float p, float (&a)[2])
 {
@@ -53,7 +65,7 @@ __device__ __forceinline__ void acc_pair(const float2 &yi, const float2 &yj, flo
 
 template <int MODE>
 __global__ void __launch_bounds__(TILE_THREADS, 4)
-k_attr_tile(int n, int ntile, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+k_attr_tile(int n, int ntile, int rows, int umax, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
             const unsigned short *__restrict__ lidx, const int *__restrict__ uptr, const int *__restrict__ ucol,
             const float2 *__restrict__ Y, float2 *__restrict__ Yn, float2 *__restrict__ uY,
             float2 *__restrict__ gains, const float2 *__restrict__ rep, const int *__restrict__ rep_flag,
@@ -66,14 +78,29 @@ k_attr_tile(int n, int ntile, const int *__restrict__ rp, const int *__restrict_
     double acc[2] = {0.0, 0.0};
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
         const int u0 = uptr[t], u = uptr[t + 1] - u0;
-        const bool staged = u <= TILE_UMAX;   // uniform over the CTA
+        const bool staged = u <= umax;        // uniform over the CTA
         __syncthreads();                      // the previous tile's reads are done
-        if (staged)
-            for (int k = tid; k < u; k += TILE_THREADS) sy[k] = __ldg(Y + __ldg(ucol + u0 + k));
+        if (staged) {
+            // column indices eight at a time, then their eight gathers issued without waiting
+            for (int k0 = tid; k0 < u; k0 += TILE_THREADS * 8) {
+                int c[8];
+#pragma unroll
+                for (int g = 0; g < 8; g++) {
+                    const int k = k0 + g * TILE_THREADS;
+                    c[g] = k < u ? __ldg(ucol + u0 + k) : 0;
+                }
+#pragma unroll
+                for (int g = 0; g < 8; g++) {
+                    const int k = k0 + g * TILE_THREADS;
+                    if (k < u) cp_async8(sy + k, Y + c[g]);
+                }
+            }
+            cp_async_wait_all();
+        }
         __syncthreads();
-        // every half-warp takes TILE_R / 16 rows, so both halves of a warp run the same rounds
-        for (int rr = hw; rr < TILE_R; rr += TILE_THREADS / 16) {
-            const int i = t * TILE_R + rr;
+        // every half-warp takes rows / 16 rows, so both halves of a warp run the same rounds
+        for (int rr = hw; rr < rows; rr += TILE_THREADS / 16) {
+            const int i = t * rows + rr;
             const bool live = i < n;
             float2 yi = make_float2(0.f, 0.f), opnd = make_float2(0.f, 0.f);
             int b = 0, e = 0;
@@ -161,12 +188,12 @@ k_attr_tile(int n, int ntile, const int *__restrict__ rp, const int *__restrict_
 }
 
 // ---- format construction ----
-__global__ void k_tile_keys(int n, const int *__restrict__ rp, const int *__restrict__ col,
+__global__ void k_tile_keys(int n, int rows, const int *__restrict__ rp, const int *__restrict__ col,
                             unsigned long long *__restrict__ keys, int *__restrict__ vals)
 {
     const int lane = threadIdx.x & 31;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-        const unsigned long long hi = (unsigned long long)(i / TILE_R) << 32;
+        const unsigned long long hi = (unsigned long long)(i / rows) << 32;
         for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) {
             keys[e] = hi | (unsigned)col[e];
             vals[e] = e;
@@ -222,15 +249,16 @@ int tile_key_bits(int ntile)
 
 }  // namespace
 
-int attr_tiles_build(cudaStream_t st, int n, long long padded_nnz, const int *rp, const int *col, AttrTiles &out)
+int attr_tiles_build(cudaStream_t st, int n, long long padded_nnz, const int *rp, const int *col, int rows, int umax,
+                     AttrTiles &out)
 {
-    if (padded_nnz + 1 > 0x7fffffffLL) return -1;
+    if (padded_nnz + 1 > 0x7fffffffLL || rows < 16 || rows % 16 != 0 || umax < 256 || umax > TILE_UMAX_CAP) return -1;
     const int m = (int)padded_nnz;
-    const int ntile = (n + TILE_R - 1) / TILE_R;
+    const int ntile = (n + rows - 1) / rows;
     DevBuf<unsigned long long> keys, keys2;
     DevBuf<int> vals, vals2, head, pos;
     keys.exact(std::max(m, 1)); vals.exact(std::max(m, 1));
-    k_tile_keys<<<148 * 8, 256, 0, st>>>(n, rp, col, keys.p, vals.p);
+    k_tile_keys<<<148 * 8, 256, 0, st>>>(n, rows, rp, col, keys.p, vals.p);
     keys2.exact(std::max(m, 1)); vals2.exact(std::max(m, 1));
     {
         size_t bytes = 0;
@@ -267,9 +295,18 @@ int attr_tiles_build(cudaStream_t st, int n, long long padded_nnz, const int *rp
     k_tile_lidx<<<148 * 8, 256, 0, st>>>(m, keys2.p, vals2.p, head.p, pos.p, out.uptr.p, out.lidx.p);
     TSNE_CUDA_CHECK(cudaGetLastError());
     out.ntile = ntile;
+    out.rows = rows;
+    out.umax = umax;
     out.n_unique = cnt;
     out.valid = true;
     return 0;
+}
+
+// persistent CTAs resident at once for a stage of umax columns (shared memory per SM 228 KB)
+static int tile_grid(int umax)
+{
+    const int per_sm = std::min(4, (228 * 1024) / (int)(sizeof(float2) * umax + 1024));
+    return 148 * std::max(1, per_sm);
 }
 
 static void set_smem_once()
@@ -277,10 +314,9 @@ static void set_smem_once()
     static bool done[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
-    TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_attr_tile<T_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TILE_SMEM));
-    TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_attr_tile<T_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TILE_SMEM));
+    const int smem = (int)(sizeof(float2) * TILE_UMAX_CAP);
+    TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_attr_tile<T_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_attr_tile<T_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     done[dev] = true;
 }
 
@@ -289,8 +325,8 @@ void launch_attr_tile_update(cudaStream_t st, int n, const AttrTiles &tl, const 
                              const int *rep_flag, float exag4, float mom, float lr, double *partials)
 {
     set_smem_once();
-    k_attr_tile<T_FUSED><<<TILE_GRID, TILE_THREADS, TILE_SMEM, st>>>(
-        n, tl.ntile, rp, col, val, tl.lidx.p, tl.uptr.p, tl.ucol.p, (const float2 *)Y, (float2 *)Ynext,
+    k_attr_tile<T_FUSED><<<tile_grid(tl.umax), TILE_THREADS, sizeof(float2) * tl.umax, st>>>(
+        n, tl.ntile, tl.rows, tl.umax, rp, col, val, tl.lidx.p, tl.uptr.p, tl.ucol.p, (const float2 *)Y, (float2 *)Ynext,
         (float2 *)uY, (float2 *)gains, (const float2 *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
 }
 
@@ -298,8 +334,8 @@ void launch_attr_tile_grad(cudaStream_t st, int n, const AttrTiles &tl, const in
                            const float *val, const void *Y, void *attr)
 {
     set_smem_once();
-    k_attr_tile<T_GRAD><<<TILE_GRID, TILE_THREADS, TILE_SMEM, st>>>(
-        n, tl.ntile, rp, col, val, tl.lidx.p, tl.uptr.p, tl.ucol.p, (const float2 *)Y, nullptr, nullptr, nullptr,
+    k_attr_tile<T_GRAD><<<tile_grid(tl.umax), TILE_THREADS, sizeof(float2) * tl.umax, st>>>(
+        n, tl.ntile, tl.rows, tl.umax, rp, col, val, tl.lidx.p, tl.uptr.p, tl.ucol.p, (const float2 *)Y, nullptr, nullptr, nullptr,
         nullptr, nullptr, 0.f, 0.f, 0.f, nullptr, (float2 *)attr);
 }
 

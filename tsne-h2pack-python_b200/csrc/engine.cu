@@ -469,10 +469,11 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
             if (*c == ',') c++;
         }
     }
-    // the shared-column tile form of the 2D attractive pass, built at the renumberings from
-    // iteration tiles_from on (TSNE_ATTR_TILES=0 keeps the CSR pass throughout)
-    const bool tiles_on = env_int("TSNE_ATTR_TILES", 1) != 0 && window_off();
+    // the shared-column tile form of the 2D attractive pass (TSNE_ATTR_TILES=1; off by default
+    // until it measures faster), built at the renumberings from iteration tiles_from on
+    const bool tiles_on = env_int("TSNE_ATTR_TILES", 0) != 0 && window_off();
     const int tiles_from = env_int("TSNE_ATTR_TILES_FROM", 100);
+    const int tile_rows = env_int("TSNE_ATTR_TILE_ROWS", 64), tile_umax = env_int("TSNE_ATTR_TILE_UMAX", 6144);
     const int h2_freq = p.h2_rebuild_freq > 0 ? p.h2_rebuild_freq : 10;
     const bool never_h2 = h2_freq > 100000;
     cudaStream_t st = ws->st;
@@ -519,7 +520,7 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
                 const double t0 = wall_sec();
                 renumber(ws, ws->h2->perm_device());
                 if (D == 2 && tiles_on && iter >= tiles_from) {
-                    attr_tiles_build(st, n, ws->padded_nnz, ws->rp.p, ws->col.p, ws->tiles);
+                    attr_tiles_build(st, n, ws->padded_nnz, ws->rp.p, ws->col.p, tile_rows, tile_umax, ws->tiles);
                     ws->n_launch += 8;
                 }
                 if (env_int("TSNE_H2_TIMERS", 0)) printf("RENUMBER iter %d %.1f ms\n", iter, 1e3 * (wall_sec() - t0));

@@ -1112,17 +1112,26 @@ k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
     __shared__ int s_crank[4], s_item;
     const TreeView &tv = g.tv;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (!LEAVES && tid == 0) s_item = atomicAdd(dp.ticket, 1);
+    // internal nodes by level (items == nullptr): one launch per level, node n_item + block,
+    // its children finished by the launches before, so nothing waits or publishes
+    const bool bylevel = !LEAVES && items == nullptr;
+    if (!LEAVES && !bylevel && tid == 0) s_item = atomicAdd(dp.ticket, 1);
     __syncthreads();
-    const int item = LEAVES ? (int)blockIdx.x : s_item;
-    if (item >= n_item) return;
-    const int t = items[LEAVES ? item : n_item - 1 - item];
+    int t;
+    if (bylevel) {
+        t = n_item + (int)blockIdx.x;
+        if (tv.leaf[t]) return;   // uniform over the CTA
+    } else {
+        const int item = LEAVES ? (int)blockIdx.x : s_item;
+        if (item >= n_item) return;
+        t = items[LEAVES ? item : n_item - 1 - item];
+    }
     const int lvl = tv.level[t];
     const float2 *xt = (const float2 *)g.xt;
     float2 *skel = (float2 *)g.skel;
     const int cfirst = tv.fchild[t], nch = LEAVES ? 0 : tv.nchild[t];
     if (!LEAVES && tid < nch) {
-        if (!tv.leaf[cfirst + tid]) dep_wait(dp, cfirst + tid);   // leaves: the launch before
+        if (!bylevel && !tv.leaf[cfirst + tid]) dep_wait(dp, cfirst + tid);   // leaves: the launch before
         s_crank[tid] = __ldcg(g.rank + cfirst + tid);
     }
     __syncthreads();
@@ -1325,7 +1334,7 @@ k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
         for (int c = 1; c < C; c++) add4(y, part[c * RG + tid]);
         g.y0[(size_t)t * MAXR + tid] = y;
     }
-    if (!LEAVES) {
+    if (!LEAVES && !bylevel) {
         __syncthreads();
         if (tid == 0) dep_publish(dp, t);
     }
@@ -1714,15 +1723,22 @@ __global__ void __launch_bounds__(DOWN_THREADS) k_down_internal(int n_item, cons
     __shared__ int s_item, s_cs[NC + 1];
     const TreeView &tv = g.tv;
     const int tid = threadIdx.x;
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(dp.ticket, 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= n_item) break;
-        const int t = items[item];
+    // by level (items == nullptr): the CTAs of one launch take the nodes n_item .. n_item +
+    // gridDim.x - 1 of one level, whose parents the launch before pushed; no waits
+    const bool bylevel = items == nullptr;
+    for (int round = 0;; round++) {
+        if (bylevel) {
+            if (round > 0) break;
+            if (tv.leaf[n_item + blockIdx.x]) break;
+        } else {
+            if (tid == 0) s_item = atomicAdd(dp.ticket, 1);
+            __syncthreads();
+            if (s_item >= n_item) break;
+        }
+        const int t = bylevel ? n_item + (int)blockIdx.x : items[s_item];
         if (tid == 0) {
             const int p = tv.parent[t];
-            if (tv.level[p] >= MIN_ADM_LEVEL) dep_wait(dp, p);
+            if (!bylevel && tv.level[p] >= MIN_ADM_LEVEL) dep_wait(dp, p);
             const int c0 = tv.fchild[t], nch = tv.nchild[t];
             int acc = 0;
             s_cs[0] = 0;
@@ -1756,7 +1772,7 @@ __global__ void __launch_bounds__(DOWN_THREADS) k_down_internal(int n_item, cons
             *dst = o;
         }
         __syncthreads();
-        if (tid == 0) dep_publish(dp, t);
+        if (tid == 0 && !bylevel) dep_publish(dp, t);
     }
 }
 
@@ -1967,7 +1983,16 @@ public:
                 k_id2d<true, ID2_THREADS><<<hbig_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hbig_, blist_.p, il, dp);
             mark_end(t_bases, 2);
             t_bases = mark_begin();
-            if (hint_ > 0) {
+            if (hint_ > 0 && id_by_level_) {
+                // one launch per level, deepest first (TSNE_ID_BYLEVEL=1)
+                for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
+                    const int nl = I.n_level_nodes[l];
+                    if (nl <= 0) continue;
+                    k_id2d<false, ID2_THREADS><<<nl, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(
+                        I.level_begin[l], nullptr, il, dp);
+                    launches_++;
+                }
+            } else if (hint_ > 0) {
                 TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
                 k_id2d<false, ID2_THREADS><<<hint_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hint_, ilist_.p, il, dp);
             }
@@ -2212,6 +2237,8 @@ private:
     static constexpr int N_PHASE = 8;
     struct Mark { cudaEvent_t a, b; int phase; };
     bool timing_ = getenv("TSNE_H2_TIMERS") && atoi(getenv("TSNE_H2_TIMERS")) != 0;
+    bool id_by_level_ = getenv("TSNE_ID_BYLEVEL") && atoi(getenv("TSNE_ID_BYLEVEL")) != 0;
+    bool down_by_level_ = getenv("TSNE_DOWN_BYLEVEL") && atoi(getenv("TSNE_DOWN_BYLEVEL")) != 0;
     std::vector<Mark> marks_;
     double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaEvent_t mark_begin()
@@ -2342,7 +2369,16 @@ private:
         mark_end(t_near, 4);
         launches_ += 2;
         cudaEvent_t t_down = mark_begin();
-        if (hint_ > 0) {
+        if (hint_ > 0 && down_by_level_) {
+            // one launch per level, top first (TSNE_DOWN_BYLEVEL=1)
+            DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
+            for (int l = MIN_ADM_LEVEL; l <= max_level_; l++) {
+                const int nl = I.n_level_nodes[l];
+                if (nl <= 0) continue;
+                k_down_internal<D><<<nl, DOWN_THREADS, 0, st_>>>(I.level_begin[l], nullptr, g, dp);
+                launches_++;
+            }
+        } else if (hint_ > 0) {
             TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
             DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
             k_down_internal<D><<<std::min(hint_, 148 * 8), DOWN_THREADS, 0, st_>>>(hint_, ilist_.p, g, dp);

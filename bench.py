@@ -92,6 +92,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=60.0, help="served: arrival window, seconds")
     ap.add_argument("--max-concurrent", type=int, default=16)
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--autotune", action="store_true",
+                    help="batched/served: each job's leaf size from the leaf-size autotuner of its size bucket")
     return ap.parse_args()
 
 
@@ -531,7 +533,7 @@ def batched(args, local):
         _serial_plain(be, inputs[i:i + 1], 50)
     clocks = Clocks(local)
     clocks.start()
-    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb) as srv:
+    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb, autotune=args.autotune) as srv:
         t0 = time.perf_counter()
         ids = [srv.submit(P, n_components=d, params=_job_params(be, P.shape[0], iters, perp, i))
                for i, (P, d, perp) in enumerate(inputs)]
@@ -548,6 +550,7 @@ def batched(args, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic: equal-cluster 50-dim float32 mixtures, seed 1234; exact k = 3 perplexity graphs",
            "config": {"workload": "batched", "jobs": len(inputs), "max_concurrent": args.max_concurrent,
+                      "autotune": bool(args.autotune),
                       "hbm_budget_gb": args.hbm_budget_gb, "iterations": iters,
                       "n_points_total": int(sum(P.shape[0] for P, _, _ in inputs))},
            "serial_plain": {"value": round(len(inputs) / wall_serial, 3), "unit": "jobs/s",
@@ -627,7 +630,7 @@ def served(args, local):
         _serial_plain(be, inputs[i:i + 1], 50)
     clocks = Clocks(local)
     clocks.start()
-    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb) as srv:
+    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb, autotune=args.autotune) as srv:
         start = time.perf_counter()
         ids = []
         for i, ((P, d, perp), at) in enumerate(zip(inputs, arrivals)):
@@ -645,6 +648,7 @@ def served(args, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic: 50-dim float32 Zipf(1.1) mixtures, seed 4321; exact k = 90 graphs",
            "config": {"workload": "served", "jobs": len(inputs), "rate": args.rate, "duration_s": args.duration,
+                      "autotune": bool(args.autotune),
                       "max_concurrent": args.max_concurrent, "hbm_budget_gb": args.hbm_budget_gb,
                       "iterations": iters},
            "latency_s": _pcts([r.latency_s for r in res]), "queue_s": _pcts([r.queue_s for r in res]),

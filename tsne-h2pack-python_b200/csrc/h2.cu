@@ -1630,8 +1630,14 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
     const int tid = threadIdx.x;
     const int s0 = tv.start[t], cnt = tv.end[t] - s0, lt = tv.level[t];
     for (int chunk = 0; chunk < cnt; chunk += NEAR2_TILE) {
-        const int a0 = chunk + tid, a1 = a0 + NEAR2_THREADS;
-        const float2 x0 = xt[s0 + (a0 < cnt ? a0 : 0)], x1 = xt[s0 + (a1 < cnt ? a1 : 0)];
+        // the chunk's m targets in pairs (tid, tid + ceil(m / 2)), so both halves of every paired
+        // instruction hold a real target (a leaf of at most 64 points would otherwise leave the
+        // second half idle); threads past the pairs only help stage the sources
+        const int m = min(NEAR2_TILE, cnt - chunk), hm = (m + 1) >> 1;
+        const bool act = tid < hm;
+        const int a0 = chunk + tid, a1 = chunk + tid + hm;
+        const bool v1 = act && a1 < chunk + m;
+        const float2 x0 = xt[s0 + (act ? a0 : chunk)], x1 = xt[s0 + (v1 ? a1 : chunk)];
         const F2 ax = f2_pack(x0.x, x1.x), ay = f2_pack(x0.y, x1.y);
         F2 acc0 = f2_pack(0.f, 0.f), accx = acc0, accy = acc0;
         for (int e = g.near_ptr[t]; e < g.near_ptr[t + 1]; e++) {
@@ -1644,7 +1650,7 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
                     sxy[b] = make_float4(p.x, p.x, p.y, p.y);
                 }
                 __syncthreads();
-                const int lim = min(NEAR2_TILE, sc - tile);
+                const int lim = act ? min(NEAR2_TILE, sc - tile) : 0;
                 if (s == t) {
                     const int self0 = a0 - tile, self1 = a1 - tile;
                     for (int j = 0; j < lim; j++) {
@@ -1684,7 +1690,7 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
                 sw2[b] = make_float2(y.z, y.z);
             }
             __syncthreads();
-            for (int b = 0; b < rs; b++) {
+            for (int b = 0; b < (act ? rs : 0); b++) {
                 const float4 q = sxy[b];
                 const float4 y01 = sw01[b];
                 const float2 y2 = sw2[b];
@@ -1698,8 +1704,8 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
         f2_unpack(acc0, c00, c01);
         f2_unpack(accx, cx0, cx1);
         f2_unpack(accy, cy0, cy1);
-        if (a0 < cnt) g.yp[s0 + a0] = make_float4(c00, cx0, cy0, 0.f);
-        if (a1 < cnt) g.yp[s0 + a1] = make_float4(c01, cx1, cy1, 0.f);
+        if (act) g.yp[s0 + a0] = make_float4(c00, cx0, cy0, 0.f);
+        if (v1) g.yp[s0 + a1] = make_float4(c01, cx1, cy1, 0.f);
     }
 }
 

@@ -246,11 +246,19 @@ __device__ __forceinline__ void tree_bits(int fm, int l, bool &bn, bool &bb)
 }
 
 template <int D>
-__global__ void __launch_bounds__(TREE_BLOCK) k_tree_marks(TreeView tv)
+__global__ void __launch_bounds__(TREE_BLOCK) k_tree_marks(TreeView tv, int window)
 {
     __shared__ int wc[2][32][TREE_BLOCK / 32];
+    extern __shared__ signed char swin[];
     const int n = tv.n, L = tv.L, leaf = tv.leaf_size;
-    const signed char *delta = tv.delta;
+    // the walks below reach at most leaf + 1 entries left and leaf right of the block's points:
+    // that window of delta is staged in shared memory when it was sized for it
+    const int w0 = max(0, (int)blockIdx.x * TREE_BLOCK - leaf - 1);
+    const int w1 = min(n, (int)blockIdx.x * TREE_BLOCK + TREE_BLOCK - 1 + leaf + 1);
+    if (window)
+        for (int j = w0 + (int)threadIdx.x; j <= w1; j += TREE_BLOCK) swin[j - w0] = tv.delta[j];
+    __syncthreads();
+    const signed char *delta = window ? swin - w0 : tv.delta;
     const int s = blockIdx.x * TREE_BLOCK + threadIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int fm = -1;
@@ -382,12 +390,16 @@ __global__ void __launch_bounds__(TREE_BLOCK) k_tree_emit(TreeView tv)
         if (lane == 0) { wo[0][l][w] = __popc(vn); wo[1][l][w] = __popc(vb); }
     }
     __syncthreads();
+    __shared__ int sboff[2][32], slb[32];
     if (threadIdx.x < 64) {   // exclusive scan over the warps, per array and level
         const int arr = threadIdx.x >> 5, l = threadIdx.x & 31;
         if (l <= L) {
             int run = 0;
             for (int k = 0; k < TREE_BLOCK / 32; k++) { const int c = wo[arr][l][k]; wo[arr][l][k] = run; run += c; }
         }
+        // the block's level offsets, read once (not once per level by every warp)
+        sboff[arr][l] = l <= L ? tv.blkoff[((size_t)blockIdx.x * 2 + arr) * 32 + l] : 0;
+        if (arr == 0) slb[l] = info->level_begin[l];
     }
     __syncthreads();
     const size_t cap = (size_t)tv.cap_node;
@@ -398,12 +410,12 @@ __global__ void __launch_bounds__(TREE_BLOCK) k_tree_emit(TreeView tv)
         bool bn, bb;
         tree_bits(fm, l, bn, bb);
         const unsigned vn = __ballot_sync(0xffffffffu, bn), vb = __ballot_sync(0xffffffffu, bb);
-        const int br = tv.blkoff[((size_t)blockIdx.x * 2 + 1) * 32 + l] + wo[1][l][w] + __popc(vb & lt);
+        const int br = sboff[1][l] + wo[1][l][w] + __popc(vb & lt);
         if (bb) {
             int id = -1;
             if (bn) {
-                const int nr = tv.blkoff[((size_t)blockIdx.x * 2 + 0) * 32 + l] + wo[0][l][w] + __popc(vn & lt);
-                id = info->level_begin[l] + nr;
+                const int nr = sboff[0][l] + wo[0][l][w] + __popc(vn & lt);
+                id = slb[l] + nr;
                 tv.start[id] = s;
                 tv.level[id] = l;
                 tv.leaf[id] = l == m ? 1 : 0;
@@ -1934,7 +1946,11 @@ public:
                                                                 perm_.p, n_, 0, D * L, st_));
                 k_gather<D><<<grid_for(n_ + 1, 256), 256, 0, st_>>>(n_, L, perm_.p, (const Vec<D> *)Y,
                                                                      (Vec<D> *)xt_.p, keys_.p, delta_.p);
-                k_tree_marks<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());
+                {
+                    const size_t win = (size_t)TREE_BLOCK + 2 * (size_t)leaf_size_ + 4;
+                    const bool staged = win <= 32 * 1024;   // with the 8 KB of counts, within the default 48 KB
+                    k_tree_marks<D><<<nblk, TREE_BLOCK, staged ? win : 0, st_>>>(view(), staged ? 1 : 0);
+                }
                 k_tree_scan<<<64, TREE_SCAN_THREADS, 0, st_>>>(nblk, view());
                 k_tree_levels<<<1, 32, 0, st_>>>(view());
                 k_tree_emit<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());

@@ -1771,72 +1771,26 @@ __device__ __forceinline__ void down_node(const ProdArgs &g, int t, int lane, fl
     __syncwarp();
 }
 
-// downward pass of every internal node at level >= 2 in one dependency-ordered launch: a CTA
-// per node (items in increasing node id, taken from the ticket counter), every candidate row
-// of the node's U (its children's skeleton slots, at most 2^D * MAXR) in flight at once, a
-// thread per row, so a node costs about one L2 round trip instead of one per 32 rows. A node
-// waits for its parent's push; the per-row sums run in the same order as down_node's.
-constexpr int DOWN_THREADS = 256;
-
+// downward pass of every internal node at level >= 2 in one dependency-ordered launch
+// (persistent warps, items in increasing node id): a node waits for its parent's push
 template <int D>
-__global__ void __launch_bounds__(DOWN_THREADS) k_down_internal(int n_item, const int *__restrict__ items,
-                                                                 ProdArgs g, DepArgs dp)
+__global__ void __launch_bounds__(256) k_down_internal(int n_item, const int *__restrict__ items, ProdArgs g,
+                                                        DepArgs dp)
 {
-    constexpr int MAXR = Dim<D>::MAXR, NC = 1 << D;
-    __shared__ float4 sy[MAXR];
-    __shared__ int s_item, s_cs[NC + 1];
-    const TreeView &tv = g.tv;
-    const int tid = threadIdx.x;
-    // by level (items == nullptr): the CTAs of one launch take the nodes n_item .. n_item +
-    // gridDim.x - 1 of one level, whose parents the launch before pushed; no waits
-    const bool bylevel = items == nullptr;
-    for (int round = 0;; round++) {
-        if (bylevel) {
-            if (round > 0) break;
-            if (tv.leaf[n_item + blockIdx.x]) break;
-        } else {
-            if (tid == 0) s_item = atomicAdd(dp.ticket, 1);
-            __syncthreads();
-            if (s_item >= n_item) break;
-        }
-        const int t = bylevel ? n_item + (int)blockIdx.x : items[s_item];
-        if (tid == 0) {
-            const int p = tv.parent[t];
-            if (!bylevel && tv.level[p] >= MIN_ADM_LEVEL) dep_wait(dp, p);
-            const int c0 = tv.fchild[t], nch = tv.nchild[t];
-            int acc = 0;
-            s_cs[0] = 0;
-            for (int c = 0; c < NC; c++) {
-                acc += c < nch ? g.rank[c0 + c] : 0;
-                s_cs[c + 1] = acc;
-            }
-        }
-        __syncthreads();
-        const int r = g.rank[t];
-        for (int k = tid; k < r; k += DOWN_THREADS) sy[k] = __ldcg(g.y1 + (size_t)t * MAXR + k);
-        __syncthreads();
-        const float *U = g.U + g.rowoff[t] * MAXR;
-        const int m = s_cs[NC], r4 = r & ~3, c0 = tv.fchild[t];
-        for (int a = tid; a < m; a += DOWN_THREADS) {
-            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-            const float *u = U + (size_t)a * MAXR;
-            for (int k = 0; k < r4; k += 4) {
-                const float4 w = *reinterpret_cast<const float4 *>(u + k);
-                fma4(acc, w.x, sy[k]);
-                fma4(acc, w.y, sy[k + 1]);
-                fma4(acc, w.z, sy[k + 2]);
-                fma4(acc, w.w, sy[k + 3]);
-            }
-            for (int k = r4; k < r; k++) fma4(acc, u[k], sy[k]);
-            int c = 0;
-            while (a >= s_cs[c + 1]) c++;
-            float4 *dst = g.y1 + (size_t)(c0 + c) * MAXR + (a - s_cs[c]);
-            float4 o = __ldcg(dst);
-            add4(o, acc);
-            *dst = o;
-        }
-        __syncthreads();
-        if (tid == 0 && !bylevel) dep_publish(dp, t);
+    __shared__ float4 sy[256 / 32][Dim<D>::MAXR];
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(dp.ticket, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= n_item) break;
+        const int t = items[item];
+        const int p = g.tv.parent[t];
+        if (lane == 0 && g.tv.level[p] >= MIN_ADM_LEVEL) dep_wait(dp, p);
+        __syncwarp();
+        down_node<D, true>(g, t, lane, sy[threadIdx.x >> 5]);
+        __syncwarp();
+        if (lane == 0) dep_publish(dp, t);
     }
 }
 
@@ -2315,7 +2269,6 @@ private:
     struct Mark { cudaEvent_t a, b; int phase; };
     bool timing_ = getenv("TSNE_H2_TIMERS") && atoi(getenv("TSNE_H2_TIMERS")) != 0;
     bool id_by_level_ = getenv("TSNE_ID_BYLEVEL") && atoi(getenv("TSNE_ID_BYLEVEL")) != 0;
-    bool down_by_level_ = getenv("TSNE_DOWN_BYLEVEL") && atoi(getenv("TSNE_DOWN_BYLEVEL")) != 0;
     std::vector<Mark> marks_;
     double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaEvent_t mark_begin()
@@ -2449,19 +2402,10 @@ private:
         mark_end(t_near, 4);
         launches_ += 2;
         cudaEvent_t t_down = mark_begin();
-        if (hint_ > 0 && down_by_level_) {
-            // one launch per level, top first (TSNE_DOWN_BYLEVEL=1)
-            DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
-            for (int l = MIN_ADM_LEVEL; l <= max_level_; l++) {
-                const int nl = I.n_level_nodes[l];
-                if (nl <= 0) continue;
-                k_down_internal<D><<<nl, DOWN_THREADS, 0, st_>>>(I.level_begin[l], nullptr, g, dp);
-                launches_++;
-            }
-        } else if (hint_ > 0) {
+        if (hint_ > 0) {
             TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
             DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
-            k_down_internal<D><<<std::min(hint_, 148 * 8), DOWN_THREADS, 0, st_>>>(hint_, ilist_.p, g, dp);
+            k_down_internal<D><<<grid_for((long long)hint_ * 32, 256, 148 * 8), 256, 0, st_>>>(hint_, ilist_.p, g, dp);
             launches_++;
         }
         k_down_leaves<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(g);

@@ -246,19 +246,11 @@ __device__ __forceinline__ void tree_bits(int fm, int l, bool &bn, bool &bb)
 }
 
 template <int D>
-__global__ void __launch_bounds__(TREE_BLOCK) k_tree_marks(TreeView tv, int window)
+__global__ void __launch_bounds__(TREE_BLOCK) k_tree_marks(TreeView tv)
 {
     __shared__ int wc[2][32][TREE_BLOCK / 32];
-    extern __shared__ signed char swin[];
     const int n = tv.n, L = tv.L, leaf = tv.leaf_size;
-    // the walks below reach at most leaf + 1 entries left and leaf right of the block's points:
-    // that window of delta is staged in shared memory when it was sized for it
-    const int w0 = max(0, (int)blockIdx.x * TREE_BLOCK - leaf - 1);
-    const int w1 = min(n, (int)blockIdx.x * TREE_BLOCK + TREE_BLOCK - 1 + leaf + 1);
-    if (window)
-        for (int j = w0 + (int)threadIdx.x; j <= w1; j += TREE_BLOCK) swin[j - w0] = tv.delta[j];
-    __syncthreads();
-    const signed char *delta = window ? swin - w0 : tv.delta;
+    const signed char *delta = tv.delta;
     const int s = blockIdx.x * TREE_BLOCK + threadIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int fm = -1;
@@ -1642,14 +1634,8 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
     const int tid = threadIdx.x;
     const int s0 = tv.start[t], cnt = tv.end[t] - s0, lt = tv.level[t];
     for (int chunk = 0; chunk < cnt; chunk += NEAR2_TILE) {
-        // the chunk's m targets in pairs (tid, tid + ceil(m / 2)), so both halves of every paired
-        // instruction hold a real target (a leaf of at most 64 points would otherwise leave the
-        // second half idle); threads past the pairs only help stage the sources
-        const int m = min(NEAR2_TILE, cnt - chunk), hm = (m + 1) >> 1;
-        const bool act = tid < hm;
-        const int a0 = chunk + tid, a1 = chunk + tid + hm;
-        const bool v1 = act && a1 < chunk + m;
-        const float2 x0 = xt[s0 + (act ? a0 : chunk)], x1 = xt[s0 + (v1 ? a1 : chunk)];
+        const int a0 = chunk + tid, a1 = a0 + NEAR2_THREADS;
+        const float2 x0 = xt[s0 + (a0 < cnt ? a0 : 0)], x1 = xt[s0 + (a1 < cnt ? a1 : 0)];
         const F2 ax = f2_pack(x0.x, x1.x), ay = f2_pack(x0.y, x1.y);
         F2 acc0 = f2_pack(0.f, 0.f), accx = acc0, accy = acc0;
         for (int e = g.near_ptr[t]; e < g.near_ptr[t + 1]; e++) {
@@ -1662,7 +1648,7 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
                     sxy[b] = make_float4(p.x, p.x, p.y, p.y);
                 }
                 __syncthreads();
-                const int lim = act ? min(NEAR2_TILE, sc - tile) : 0;
+                const int lim = min(NEAR2_TILE, sc - tile);
                 if (s == t) {
                     const int self0 = a0 - tile, self1 = a1 - tile;
                     for (int j = 0; j < lim; j++) {
@@ -1702,7 +1688,7 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
                 sw2[b] = make_float2(y.z, y.z);
             }
             __syncthreads();
-            for (int b = 0; b < (act ? rs : 0); b++) {
+            for (int b = 0; b < rs; b++) {
                 const float4 q = sxy[b];
                 const float4 y01 = sw01[b];
                 const float2 y2 = sw2[b];
@@ -1716,8 +1702,8 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
         f2_unpack(acc0, c00, c01);
         f2_unpack(accx, cx0, cx1);
         f2_unpack(accy, cy0, cy1);
-        if (act) g.yp[s0 + a0] = make_float4(c00, cx0, cy0, 0.f);
-        if (v1) g.yp[s0 + a1] = make_float4(c01, cx1, cy1, 0.f);
+        if (a0 < cnt) g.yp[s0 + a0] = make_float4(c00, cx0, cy0, 0.f);
+        if (a1 < cnt) g.yp[s0 + a1] = make_float4(c01, cx1, cy1, 0.f);
     }
 }
 
@@ -1900,11 +1886,7 @@ public:
                                                                 perm_.p, n_, 0, D * L, st_));
                 k_gather<D><<<grid_for(n_ + 1, 256), 256, 0, st_>>>(n_, L, perm_.p, (const Vec<D> *)Y,
                                                                      (Vec<D> *)xt_.p, keys_.p, delta_.p);
-                {
-                    const size_t win = (size_t)TREE_BLOCK + 2 * (size_t)leaf_size_ + 4;
-                    const bool staged = win <= 32 * 1024;   // with the 8 KB of counts, within the default 48 KB
-                    k_tree_marks<D><<<nblk, TREE_BLOCK, staged ? win : 0, st_>>>(view(), staged ? 1 : 0);
-                }
+                k_tree_marks<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());
                 k_tree_scan<<<64, TREE_SCAN_THREADS, 0, st_>>>(nblk, view());
                 k_tree_levels<<<1, 32, 0, st_>>>(view());
                 k_tree_emit<D><<<nblk, TREE_BLOCK, 0, st_>>>(view());

@@ -43,13 +43,15 @@ sys.path.insert(0, str(ROOT / "tsne-h2pack-python_b200"))
 METRIC = "opt-phase s at 1M pts 2D"
 
 
-def metric_name(n, iters):
+def metric_name(n, iters, d=2):
     """The headline metric for the default workload; other sizes name their own."""
-    return METRIC if (n, iters) == (1_000_000, 1000) else f"opt-phase s at {n:,} pts 2D, {iters} iterations"
+    if (n, iters, d) == (1_000_000, 1000, 2):
+        return METRIC
+    return f"opt-phase s at {n:,} pts {d}D" + ("" if iters == 1000 else f", {iters} iterations")
 
 
-def data_desc(n):
-    return f"synthetic: {n:,} x 50 float32 Zipf(1.1) Gaussian mixture, seed 1; exact k=90 graph"
+def data_desc(n, seed=1):
+    return f"synthetic: {n:,} x 50 float32 Zipf(1.1) Gaussian mixture, seed {seed}; exact k=90 graph"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 # ncu summary of the roofline kernel on a smaller case; its DRAM traffic per algorithmic byte
 # scales the traffic to this workload's launch
@@ -77,6 +79,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--dim", type=int, default=2, choices=[2, 3], help="embedding dimension (plain workload)")
+    ap.add_argument("--h2-tol", type=float, default=None, help="default 1e-2 in 2D, 3e-2 in 3D")
+    ap.add_argument("--seed", type=int, default=None, help="mixture seed: default 1 in 2D, 2 in 3D")
     ap.add_argument("--iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-runs", type=int, default=1, help="reference arm: whole runs timed")
@@ -94,7 +99,12 @@ def parse():
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     ap.add_argument("--autotune", action="store_true",
                     help="batched/served: each job's leaf size from the leaf-size autotuner of its size bucket")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.h2_tol is None:
+        args.h2_tol = 1e-2 if args.dim == 2 else 3e-2
+    if args.seed is None:
+        args.seed = 1 if args.dim == 2 else 2
+    return args
 
 
 def workload(n, seed=1, device=0, cache=None):
@@ -117,13 +127,13 @@ def workload(n, seed=1, device=0, cache=None):
     return X, G, P
 
 
-def params_for(be, n, iters):
+def params_for(be, n, iters, h2_tol=1e-2):
     p = be.create_default_params()
     p.n_iter = iters
     p.verbose = 0
     p.perplexity = 30.0
     p.learning_rate = max(n / 12.0, 200.0)
-    p.h2_tol, p.h2_rebuild_freq, p.h2_rebuild_freq_early, p.h2_leaf_size = 1e-2, 3, 10, 100
+    p.h2_tol, p.h2_rebuild_freq, p.h2_rebuild_freq_early, p.h2_leaf_size = h2_tol, 3, 10, 100
     p.random_seed = 1
     p.init_method = 0
     return p
@@ -190,16 +200,16 @@ def ours(args, rank, world, local):
     lib = be._lib
     lib.tsne_get_timing.argtypes = [ctypes.POINTER(TSNEWorkspace), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
-    n = args.n
+    n, d = args.n, args.dim
     t0 = time.time()
-    X, G, P = workload(n, device=local, cache=args.graph_cache)
+    X, G, P = workload(n, seed=args.seed, device=local, cache=args.graph_cache)
     setup_s = time.time() - t0
     nnz = P.nnz
-    Yout = np.zeros((2, n))
+    Yout = np.zeros((d, n))
 
     def step():
         """One e2e step through the C ABI; returns (wall s, device run s, attr ms, attr launches, launches)."""
-        prm = params_for(be, n, args.iters)
+        prm = params_for(be, n, args.iters, args.h2_tol)
         if args.profile_csv:
             prm.enable_profiling = 1
             prm.profiling_output_file = args.profile_csv.encode()
@@ -207,7 +217,7 @@ def ours(args, rank, world, local):
         w0 = time.perf_counter()
         Pc = scipy_csr_to_c_sparse_matrix(P, lib)
         w1 = time.perf_counter()
-        ws = lib.tsne_init_with_P(None, n, 0, 2, ctypes.byref(prm), Pc)
+        ws = lib.tsne_init_with_P(None, n, 0, d, ctypes.byref(prm), Pc)
         if not ws:
             raise RuntimeError("tsne_init_with_P returned NULL")
         w2 = time.perf_counter()
@@ -238,10 +248,10 @@ def ours(args, rank, world, local):
         import oracle as O
         with tempfile.TemporaryDirectory() as td:
             f = Path(td) / "stages.csv"
-            prm = params_for(be, n, args.iters)
+            prm = params_for(be, n, args.iters, args.h2_tol)
             prm.enable_profiling = 1
             prm.profiling_output_file = str(f).encode()
-            ws = lib.tsne_init_with_P(None, n, 0, 2, ctypes.byref(prm), scipy_csr_to_c_sparse_matrix(P, lib))
+            ws = lib.tsne_init_with_P(None, n, 0, d, ctypes.byref(prm), scipy_csr_to_c_sparse_matrix(P, lib))
             if not ws or lib.tsne_run(ws) != 0:
                 raise RuntimeError("profiled run failed")
             lib.tsne_destroy(ws)
@@ -283,19 +293,19 @@ def ours(args, rank, world, local):
         peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
         peak = peaks.get("hbm_gbs", 6650.0)
         peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-        attr_bytes = 8.0 * (nnz) + 4.0 * (n + 1) + 28.0 * 2 * n
+        attr_bytes = 8.0 * (nnz) + 4.0 * (n + 1) + 28.0 * d * n
         achieved = attr_bytes / (attr_ms * 1e-3) / 1e9
-        ratio = traffic_ratio()
+        ratio = traffic_ratio() if d == 2 else None   # the committed capture is of the 2D kernel
         traffic = round(ratio * attr_bytes) if ratio else None
-        h2d = 4 * (n + 1) + 12 * nnz + 16 * n
-        d2h = 16 * n + 8
+        h2d = 4 * (n + 1) + 12 * nnz + 8 * d * n
+        d2h = 8 * d * n + 8
         out = {
-            "metric": metric_name(n, args.iters), "value": round(dev_s, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+            "metric": metric_name(n, args.iters, d), "value": round(dev_s, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev_s * 1e3, 2), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": data_desc(n),
-            "config": {"workload": f"{n:,} points x 50 dims -> 2D, {args.iters} iterations, perplexity 30, "
-                                   "h2_tol 1e-2, H2 rebuild every 3 (10 early), leaf 100, init random",
+            "data": data_desc(n, args.seed),
+            "config": {"workload": f"{n:,} points x 50 dims -> {d}D, {args.iters} iterations, perplexity 30, "
+                                   f"h2_tol {args.h2_tol:g}, H2 rebuild every 3 (10 early), leaf 100, init random",
                        "n_points": n, "nnz_P": int(nnz), "iterations": args.iters,
                        "l2": f"inputs larger than L2 (P streams {8 * nnz / 1e9:.2f} GB per iteration)",
                        "parallelism": "replicas" if world > 1 else "single"},
@@ -315,7 +325,7 @@ def ours(args, rank, world, local):
         }
         if ck:
             out["clocks"] = ck
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and world == 1 and d == 2:
             cb, Y_ref, kl_ref = cpu_sample(P, n, args.iters)
             out["cpu_baseline"] = cb
             if Y_ref is not None:
@@ -691,6 +701,9 @@ def reference(args, rank, world, local):
     --warmup ask, and says so in the line."""
     if rank != 0:
         return None
+    if args.dim != 2:
+        return {"impl": "reference", "metric": metric_name(args.n, args.iters, args.dim),
+                "unavailable": "the reference arm times the 2D workload (the headline metric)"}
     n = args.n
     X, G, P = workload(n, device=local, cache=args.graph_cache)
     ref_full_run(P, n, args.iters, warm=True)

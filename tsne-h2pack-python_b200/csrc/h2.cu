@@ -468,6 +468,7 @@ struct DepArgs {
     int *err;       // set when a wait gave up
     int epoch;
     int limit = DEP_WAIT_LIMIT;   // polls before a wait gives up
+    int *flag2 = nullptr;         // a second per-node flag (launches that publish twice)
 };
 
 __device__ __forceinline__ int ld_acquire_gpu(const int *p)
@@ -495,6 +496,20 @@ __device__ __forceinline__ void dep_publish(const DepArgs &dp, int node)
 {
     __threadfence();
     st_release_gpu(dp.flag + node, dp.epoch);
+}
+
+// the second flag of a node (launches that publish twice: the bases publish the skeleton and
+// rank first, the upward coefficients last)
+__device__ __forceinline__ void dep_wait_y0(const DepArgs &dp, int node)
+{
+    DepArgs d2 = dp;
+    d2.flag = dp.flag2;
+    dep_wait(d2, node);
+}
+__device__ __forceinline__ void dep_publish_y0(const DepArgs &dp, int node)
+{
+    __threadfence();
+    st_release_gpu(dp.flag2 + node, dp.epoch);
 }
 
 // one bounded wait for `node` (the failure path of the dependency-ordered launches, for tests)
@@ -737,9 +752,11 @@ __global__ void __launch_bounds__(256) k_lists_compact(TreeView tv, ListOut lo)
 
 // rows of each node's interpolation matrix: a leaf's points, or (upper bound) the
 // children's skeletons; nodes above MIN_ADM_LEVEL are not compressed
-// iflag / lflag / bflag: 1 for the internal nodes / leaves of at most LEAF_SMALL points / larger
-// leaves at level >= MIN_ADM_LEVEL (the items of the basis launches)
+// iflag / lflag / bflag: 1 for the internal nodes / leaves of at most LEAF_SMALL (3D:
+// ID3_TINY_LEAF) points / larger leaves at level >= MIN_ADM_LEVEL (the items of the basis
+// launches)
 constexpr int LEAF_SMALL = 64;
+constexpr int ID3_TINY_LEAF = 32;   // 3D: the leaves of the smallest basis CTAs
 template <int D>
 __global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap, int *__restrict__ iflag, int *__restrict__ lflag,
                          int *__restrict__ bflag)
@@ -752,8 +769,9 @@ __global__ void k_rowcap(TreeView tv, int *__restrict__ rowcap, int *__restrict_
         if (adm) r = tv.leaf[t] ? tv.end[t] - tv.start[t] : NCH * Dim<D>::MAXR;
         rowcap[t] = r;
         iflag[t] = adm && !tv.leaf[t];
-        lflag[t] = adm && tv.leaf[t] && r <= LEAF_SMALL;
-        bflag[t] = adm && tv.leaf[t] && r > LEAF_SMALL;
+        const int small = D == 2 ? LEAF_SMALL : ID3_TINY_LEAF;
+        lflag[t] = adm && tv.leaf[t] && r <= small;
+        bflag[t] = adm && tv.leaf[t] && r > small;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) { rowcap[n_node] = 0; iflag[n_node] = 0; lflag[n_node] = 0; bflag[n_node] = 0; }
 }
@@ -1125,8 +1143,9 @@ __device__ __forceinline__ void warp_argmax(float &bv, int &bi)
 // most 64 points, which fit seven to an SM, and of 128 for the others). Otherwise every
 // internal node in one dependency-ordered launch (candidates = the children's skeletons):
 // items in decreasing node id (deepest level first), so a node's internal children come
-// before it; it waits for their flags and reads their ranks, skeletons and coefficients
-// through L2 (CTAs of 128 threads). When the children's ranks add up to more than 128, thread
+// before it; it waits for their first flags (skeleton and rank, published right after their
+// Gram-Schmidt steps) and, before its own upward sums, for their second flags (coefficients,
+// published last), and reads all of these through L2 (CTAs of 128 threads). When the children's ranks add up to more than 128, thread
 // tid also owns row 128 + tid, kept in global memory (in the node's first U rows, unused until
 // the end).
 // Column-pivoted Gram-Schmidt until the largest residual row norm is <= tol * the largest
@@ -1207,7 +1226,7 @@ k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
             int c = 0, aa = a;
             while (aa >= s_crank[c]) { aa -= s_crank[c]; c++; }
             pt = __ldcg(skel + (size_t)(cfirst + c) * MAXR + aa);
-            sin_[a] = __ldcg(g.y0 + (size_t)(cfirst + c) * MAXR + aa);
+            if (bylevel) sin_[a] = __ldcg(g.y0 + (size_t)(cfirst + c) * MAXR + aa);
         }
         sxy[a] = pt;
     }
@@ -1337,6 +1356,20 @@ k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
                                                                  : U[(size_t)pr * MAXR + k]);
     }
     __syncthreads();
+    // the skeleton and the rank are what the parent's decomposition needs: published here;
+    // the children's upward coefficients, published last, are waited for before the sums
+    if (!LEAVES && !bylevel) {
+        if (tid == 0) dep_publish(dp, t);
+        if (tid < nch && !tv.leaf[cfirst + tid]) dep_wait_y0(dp, cfirst + tid);
+        __syncthreads();
+        for (int q = 0; q < 2; q++) {
+            const int a = tid + THREADS * q;
+            if (a >= m) break;
+            int c = 0, aa = a;
+            while (aa >= s_crank[c]) { aa -= s_crank[c]; c++; }
+            sin_[a] = __ldcg(g.y0 + (size_t)(cfirst + c) * MAXR + aa);
+        }
+    }
     // back substitution of the non-pivot rows, column by column (independent updates)
     if (pos == -1) {
         for (int k = r - 1; k >= 0; k--) {
@@ -1386,7 +1419,442 @@ k_id2d(int n_item, const int *__restrict__ items, IdArgs g, DepArgs dp)
     }
     if (!LEAVES && !bylevel) {
         __syncthreads();
+        if (tid == 0) dep_publish_y0(dp, t);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// 3D interpolative decompositions with recomputed rows
+// ---------------------------------------------------------------------------------
+// The 3D proxy matrix has 216 columns and up to 512 candidate rows (eight children of rank
+// <= 64): 442 KB in FP32, more than one SM holds. Its entries are cheap to recompute, one
+// reciprocal each in the expanded form (1 + |x|^2 + |p|^2 - 2 x.p)^-2 (x: candidate relative
+// to the node's centre, p: proxy), so no row is stored: the column-pivoted Gram-Schmidt runs
+// left-looking. Step r takes the row b of the largest residual norm and orthonormalises it
+// against the earlier directions q_0..q_{r-1} by classical Gram-Schmidt applied twice (the
+// first pass from b's stored projections, the second recomputed, so the directions stay
+// orthonormal to rounding); every other row a then recomputes its entries once for its dot
+// product c = a . q_r (= its residual's, as q_r is orthogonal to the earlier directions),
+// kept in shared memory as R12, with its squared residual norm downdated in FP64 by c^2.
+// R11's column r is b's projections on q_0..q_{r-1} and its residual norm. The stop rule, tie
+// rule, back substitution U = [I ; R11^-1 R12]^T and the upward coefficients are those of k_id.
+//
+// One CTA per node, in three sizes (THREADS, ROWS = the most candidate rows it takes): 512
+// threads and 512 rows (internal nodes, leaves above 128 points; one CTA per SM), 256 and 128
+// (leaves of 33..128 points; two per SM), 128 and 32 (leaves of at most 32 points, four per
+// SM). The proxies are held in pairs (2j, 2j + 1) for the paired FP32 instructions; a row is
+// split over S adjacent lanes (the largest S <= 16 with THREADS / S >= rows, else 2), lane
+// `sub` taking the pairs j = sub mod S, and lane group g = tid / S covers the rows
+// g + (THREADS / S) k; the S partial sums of a row meet by butterfly shuffles, which give
+// every lane of the group the same value.
+//
+// Internal nodes run in one dependency-ordered launch: a node waits for its internal
+// children's skeletons and ranks (flag), published right after their pivot loop, and, before
+// its upward coefficients, for their coefficients (second flag, published last).
+constexpr int ID3_P = Dim<3>::NPROXY;
+constexpr int ID3_ROWS = 8 * Dim<3>::MAXR;   // candidate rows of an internal node
+constexpr int ID3_QS = 220;                  // row stride of the directions (16-byte rows,
+                                             // conflict-free for 4 lanes x 8 directions)
+constexpr int ID3_TINY = 32;                 // leaves of the 128-thread CTAs
+constexpr int ID3_SMALL = 128;               // leaves of the 256-thread CTAs
+static_assert(ID3_TINY == ID3_TINY_LEAF, "the small-leaf list is the 128-thread launch's");
+static_assert(ID3_P % 8 == 0 && ID3_QS >= ID3_P && ID3_QS % 4 == 0, "proxy pairs, 16-byte rows");
+
+template <int THREADS, int ROWS>
+struct Id3 {
+    static constexpr int QR = ROWS < Dim<3>::MAXR ? ROWS : Dim<3>::MAXR;   // rank bound
+    static constexpr int CS = QR + 1;                                      // row stride of R12 / U
+    static constexpr int NW = THREADS / 32;
+    static constexpr int NKMAX = 2 * ROWS > THREADS ? 2 * ROWS / THREADS : 1;   // rows per lane group
+    static constexpr int SMIN = THREADS >= 2 * ROWS ? THREADS / ROWS : 2;       // smallest lane split
+    static_assert(NKMAX <= 2 && THREADS >= 4 * QR, "row groups, four lanes per direction");
+    struct Smem {
+        float Q[QR * ID3_QS];                  // directions q_0..q_{r-1}; at the end: y0 partials
+        float C[ROWS * CS];                    // R12 (the rows' dots), then U
+        float4 pa[ID3_P / 2];                  // proxy pairs: (-2x, -2x', -2y, -2y')
+        float4 pb[ID3_P / 2];                  //              (-2z, -2z', |p|^2, |p'|^2)
+        float4 cand[ROWS];                     // candidates: (x, y, z) - centre, 1 + |.|^2
+        float R11[QR * (QR + 1) / 2];          // column j at j (j + 1) / 2
+        float res[ID3_P];                      // the pivot's residual
+        float dc[QR];                          // its second-pass projections
+        int piv[QR];
+        int selpos[ROWS];                      // pivot position of each row, or -1
+        float bv[2][NW];
+        int bi[2][NW];
+        float red[NW];
+        int coff[9];
+        int item;
+    };
+    static_assert(QR * ID3_QS * sizeof(float) >= THREADS * sizeof(float4), "y0 partials in the directions");
+};
+
+// entry of proxy p (scalar form of the paired arithmetic below: the same operations in the
+// same order, so both give the same value)
+template <typename SM>
+__device__ __forceinline__ float id3_entry(const SM &s, const float4 &c, int p)
+{
+    const float4 A = s.pa[p >> 1], B = s.pb[p >> 1];
+    const bool o = p & 1;
+    const float mx = o ? A.y : A.x, my = o ? A.w : A.z, mz = o ? B.y : B.x, e = o ? B.w : B.z;
+    const float d = fmaf(c.z, mz, fmaf(c.y, my, fmaf(c.x, mx, c.w + e)));
+    const float w = fast_rcp(d);
+    return w * w;
+}
+
+// Over the lane's share of the proxies (pairs sub, sub + S, ...), for its NK rows
+// g + RPG k: NORM: sum of squared entries (FP64); otherwise the dot product with v (FP32,
+// two partial sums per row).
+template <int S, int NK, bool NORM, typename SM>
+__device__ __forceinline__ void id3_rows(const SM &s, const float *v, int g, int rpg, int sub, double (&out)[2])
+{
+    F2 cx[NK], cy[NK], cz[NK], cw[NK], acc[NK];
+    double dn[NK];
+#pragma unroll
+    for (int k = 0; k < NK; k++) {
+        const float4 c = s.cand[g + rpg * k];
+        cx[k] = f2_pack(c.x, c.x); cy[k] = f2_pack(c.y, c.y); cz[k] = f2_pack(c.z, c.z); cw[k] = f2_pack(c.w, c.w);
+        acc[k] = f2_pack(0.f, 0.f);
+        dn[k] = 0.0;
+    }
+#pragma unroll 2
+    for (int j = sub; j < ID3_P / 2; j += S) {
+        const float4 A = s.pa[j], B = s.pb[j];
+        const F2 mx = f2_pack(A.x, A.y), my = f2_pack(A.z, A.w), mz = f2_pack(B.x, B.y), e = f2_pack(B.z, B.w);
+        F2 vv;
+        if (!NORM) {
+            const float2 v2 = *reinterpret_cast<const float2 *>(v + 2 * j);
+            vv = f2_pack(v2.x, v2.y);
+        }
+#pragma unroll
+        for (int k = 0; k < NK; k++) {
+            const F2 d = f2_fma(cz[k], mz, f2_fma(cy[k], my, f2_fma(cx[k], mx, f2_add(cw[k], e))));
+            float d0, d1;
+            f2_unpack(d, d0, d1);
+            const F2 w = f2_pack(fast_rcp(d0), fast_rcp(d1));
+            const F2 w2 = f2_mul(w, w);
+            if (NORM) {
+                float a0, a1;
+                f2_unpack(w2, a0, a1);
+                dn[k] = fma((double)a0, (double)a0, dn[k]);
+                dn[k] = fma((double)a1, (double)a1, dn[k]);
+            } else {
+                acc[k] = f2_fma(w2, vv, acc[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NK; k++) {
+        if (NORM) out[k] = dn[k];
+        else {
+            float a0, a1;
+            f2_unpack(acc[k], a0, a1);
+            out[k] = (double)(a0 + a1);
+        }
+    }
+}
+
+// the lane group's row sums (every lane of the group gets the same values)
+template <bool NORM, int SMIN, int NKMAX, typename SM>
+__device__ __forceinline__ void id3_rows_any(const SM &s, const float *v, int S, int g, int rpg, int sub, int nk,
+                                             double (&out)[2])
+{
+    out[0] = out[1] = 0.0;
+    if (nk > 0) {
+        if (S == 16) id3_rows<16, 1, NORM>(s, v, g, rpg, sub, out);
+        else if (S == 8) id3_rows<8, 1, NORM>(s, v, g, rpg, sub, out);
+        else if (SMIN <= 4 && S == 4) id3_rows<4, 1, NORM>(s, v, g, rpg, sub, out);
+        else if constexpr (SMIN <= 2) {
+            if (NKMAX >= 2 && nk == 2) id3_rows<2, (NKMAX >= 2 ? 2 : 1), NORM>(s, v, g, rpg, sub, out);
+            else id3_rows<2, 1, NORM>(s, v, g, rpg, sub, out);
+        }
+    }
+    for (int o = 1; o < S; o <<= 1) {
+        out[0] += __shfl_xor_sync(0xffffffffu, out[0], o);
+        out[1] += __shfl_xor_sync(0xffffffffu, out[1], o);
+    }
+}
+
+// d[j] = q_j . res for the directions j < r (four lanes per direction, 54 proxies each)
+template <typename SM>
+__device__ __forceinline__ void id3_proj(SM &s, int r, int tid, float *d)
+{
+    const int j = tid >> 2, sub = tid & 3;
+    float d0 = 0.f, d1 = 0.f;
+    if (j < r) {
+        const float *qj = s.Q + j * ID3_QS;
+#pragma unroll
+        for (int i = 0; i < ID3_P / 8; i++) {
+            const int p = sub + 8 * i;
+            d0 = fmaf(qj[p], s.res[p], d0);
+            d1 = fmaf(qj[p + 4], s.res[p + 4], d1);
+        }
+    }
+    float x = d0 + d1;
+    x += __shfl_xor_sync(0xffffffffu, x, 1);
+    x += __shfl_xor_sync(0xffffffffu, x, 2);
+    if (sub == 0 && j < r) d[j] = x;
+}
+
+// v - sum_{j < r} d[j] q_j[p]
+__device__ __forceinline__ float id3_sub(const float *Q, int r, int p, const float *d, float v)
+{
+    float a0 = v, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    int j = 0;
+    for (; j + 3 < r; j += 4) {
+        a0 = fmaf(-d[j], Q[j * ID3_QS + p], a0);
+        a1 = fmaf(-d[j + 1], Q[(j + 1) * ID3_QS + p], a1);
+        a2 = fmaf(-d[j + 2], Q[(j + 2) * ID3_QS + p], a2);
+        a3 = fmaf(-d[j + 3], Q[(j + 3) * ID3_QS + p], a3);
+    }
+    for (; j < r; j++) a0 = fmaf(-d[j], Q[j * ID3_QS + p], a0);
+    return (a0 + a1) + (a2 + a3);
+}
+
+template <int THREADS>
+constexpr int id3_min_blocks() { return THREADS >= 512 ? 1 : (THREADS >= 256 ? 2 : 4); }
+
+// LEAVES: the leaves of `items` with mlo < points <= ROWS (others are another launch's).
+template <bool LEAVES, int THREADS, int ROWS>
+__global__ void __launch_bounds__(THREADS, id3_min_blocks<THREADS>())
+k_id3(int n_item, const int *__restrict__ items, int mlo, IdArgs g, DepArgs dp)
+{
+    using K = Id3<THREADS, ROWS>;
+    using SM = typename K::Smem;
+    constexpr int P = ID3_P, MAXR = Dim<3>::MAXR, QR = K::QR, CS = K::CS, NW = K::NW;
+    constexpr int PPT = (P + THREADS - 1) / THREADS;   // proxies per thread in the pivot's steps
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SM &s = *reinterpret_cast<SM *>(smraw);
+    const TreeView &tv = g.tv;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (!LEAVES && tid == 0) s.item = atomicAdd(dp.ticket, 1);
+    __syncthreads();
+    const int item = LEAVES ? (int)blockIdx.x : s.item;
+    if (item >= n_item) return;
+    const int t = items[LEAVES ? item : n_item - 1 - item];
+    if (LEAVES) {
+        const int mm = tv.end[t] - tv.start[t];
+        if (mm <= mlo || mm > ROWS) return;   // uniform over the CTA
+    }
+    const int cfirst = tv.fchild[t], nch = LEAVES ? 0 : tv.nchild[t];
+    if (!LEAVES && tid < nch && !tv.leaf[cfirst + tid]) dep_wait(dp, cfirst + tid);
+    __syncthreads();
+    if (tid == 0) {
+        int acc = 0;
+        for (int c = 0; c < nch; c++) {
+            s.coff[c] = acc;
+            acc += __ldcg(g.rank + cfirst + c);
+        }
+        s.coff[nch] = acc;
+    }
+    __syncthreads();
+    const int m = LEAVES ? tv.end[t] - tv.start[t] : s.coff[nch];
+    const int s0 = tv.start[t];
+    const int lvl = tv.level[t];
+    const long long roff = g.rowoff[t];
+    float *U = g.U + roff * MAXR;
+    const float4 *xt = (const float4 *)g.xt;
+    float4 *skel = (float4 *)g.skel;
+    const double h = tv.info->radius / (double)(1LL << lvl);
+    float ctr[3];
+    for (int k = 0; k < 3; k++)
+        ctr[k] = (float)(tv.info->corner[k] + (double)(2 * tv.ix[(size_t)t * 3 + k] + 1) * h);
+    for (int j = tid; j < P / 2; j += THREADS) {
+        float p0[3], p1[3];
+        proxy_point<3>(2 * j, h, p0);
+        proxy_point<3>(2 * j + 1, h, p1);
+        s.pa[j] = make_float4(-2.f * p0[0], -2.f * p1[0], -2.f * p0[1], -2.f * p1[1]);
+        s.pb[j] = make_float4(-2.f * p0[2], -2.f * p1[2], fmaf(p0[0], p0[0], fmaf(p0[1], p0[1], p0[2] * p0[2])),
+                              fmaf(p1[0], p1[0], fmaf(p1[1], p1[1], p1[2] * p1[2])));
+    }
+    for (int a = tid; a < m; a += THREADS) {
+        float4 x;
+        if (LEAVES) x = xt[s0 + a];
+        else {
+            int c = 0;
+            while (a >= s.coff[c + 1]) c++;
+            x = __ldcg(skel + (size_t)(cfirst + c) * MAXR + (a - s.coff[c]));
+        }
+        const float rx = x.x - ctr[0], ry = x.y - ctr[1], rz = x.z - ctr[2];
+        s.cand[a] = make_float4(rx, ry, rz, 1.f + fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+        s.selpos[a] = -1;
+    }
+    __syncthreads();
+
+    int S = 2;   // uniform over the CTA
+    while (S < 16 && THREADS / (2 * S) >= m) S <<= 1;
+    const int rpg = THREADS / S, sub = tid & (S - 1), rb = tid / S;
+    const int nk = max(0, min(K::NKMAX, (m - rb + rpg - 1) / rpg));   // rows rb + rpg k < m
+    double nrm[2];
+    int pos[2];   // -1: open row, -2: no row, >= 0: pivot position
+    id3_rows_any<true, K::SMIN, K::NKMAX>(s, nullptr, S, rb, rpg, sub, nk, nrm);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        pos[k] = k < nk ? -1 : -2;
+        if (pos[k] == -2) nrm[k] = -1.0;
+    }
+    float bv = -1.f, lmax = 0.f;
+    int bi = INT_MAX;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float v = (float)nrm[k];
+        if (pos[k] == -1 && sub == 0 && v > bv) { bv = v; bi = rb + rpg * k; }
+        lmax = fmaxf(lmax, v);
+    }
+    lmax = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(lmax)));
+    warp_argmax(bv, bi);
+    if (lane == 0) { s.red[wid] = lmax; s.bv[0][wid] = bv; s.bi[0][wid] = bi; }
+    __syncthreads();
+    float n0 = 0.f;
+    for (int w = 0; w < NW; w++) n0 = fmaxf(n0, s.red[w]);
+    const float stop2 = g.tol2 * n0;
+    const int rmax = min(min(m, P), QR);
+    int r = 0, buf = 0;
+    while (r < rmax) {
+        float v = s.bv[buf][0];
+        int best = s.bi[buf][0];
+        for (int w = 1; w < NW; w++)
+            if (s.bv[buf][w] > v || (s.bv[buf][w] == v && s.bi[buf][w] < best)) { v = s.bv[buf][w]; best = s.bi[buf][w]; }
+        if (best == INT_MAX || !(v > stop2) || !(v > 0.f)) break;
+        // the pivot's residual: thread tid takes the proxies tid + THREADS i
+        const float *cb = s.C + best * CS;   // the pivot's projections on q_0..q_{r-1}
+        float rv[PPT];
+#pragma unroll
+        for (int i = 0; i < PPT; i++) {
+            const int p = tid + THREADS * i;
+            rv[i] = 0.f;
+            if (p < P) {
+                rv[i] = id3_sub(s.Q, r, p, cb, id3_entry(s, s.cand[best], p));
+                s.res[p] = rv[i];
+            }
+        }
+        __syncthreads();
+        if (r > 0) id3_proj(s, r, tid, s.dc);   // uniform
+        __syncthreads();
+        float sq = 0.f;
+#pragma unroll
+        for (int i = 0; i < PPT; i++) {
+            const int p = tid + THREADS * i;
+            if (p < P) {
+                rv[i] = id3_sub(s.Q, r, p, s.dc, rv[i]);
+                s.res[p] = rv[i];
+                sq = fmaf(rv[i], rv[i], sq);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if (lane == 0) s.red[wid] = sq;
+        __syncthreads();
+        float rr2 = 0.f;
+        for (int w = 0; w < NW; w++) rr2 += s.red[w];
+        const float rr = sqrtf(rr2);
+        if (!(rr > 0.f) || !(rr < INFINITY)) break;   // uniform: every thread sums the same values
+        const float inv = 1.0f / rr;
+#pragma unroll
+        for (int i = 0; i < PPT; i++)
+            if (tid + THREADS * i < P) s.Q[r * ID3_QS + tid + THREADS * i] = rv[i] * inv;
+        if (tid < r) s.R11[r * (r + 1) / 2 + tid] = cb[tid] + s.dc[tid];
+        if (tid == r) s.R11[r * (r + 1) / 2 + r] = rr;
+        if (tid == 0) { s.piv[r] = best; s.selpos[best] = r; }
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+            if (pos[k] == -1 && rb + rpg * k == best) { pos[k] = r; nrm[k] = -1.0; }
+        // every open row: c = a . q_r (from the unscaled residual), its R12 entry; squared
+        // residual norm -= c^2
+        double part[2];
+        id3_rows_any<false, K::SMIN, K::NKMAX>(s, s.res, S, rb, rpg, sub, nk, part);
+        bv = -1.f;
+        bi = INT_MAX;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float c = (float)part[k] * inv;
+            if (pos[k] == -1) {
+                nrm[k] = fmax(nrm[k] - (double)c * (double)c, 0.0);
+                if (sub == 0) {
+                    s.C[(rb + rpg * k) * CS + r] = c;
+                    const float nv = (float)nrm[k];
+                    if (nv > bv) { bv = nv; bi = rb + rpg * k; }
+                }
+            }
+        }
+        warp_argmax(bv, bi);
+        buf ^= 1;
+        if (lane == 0) { s.bv[buf][wid] = bv; s.bi[buf][wid] = bi; }
+        r++;
+        __syncthreads();
+    }
+    __syncthreads();
+    // skeleton and rank, published before the rest (the parent's candidates)
+    for (int k = tid; k < r; k += THREADS) {
+        const int a = s.piv[k];
+        float4 x;
+        if (LEAVES) x = xt[s0 + a];
+        else {
+            int c = 0;
+            while (a >= s.coff[c + 1]) c++;
+            x = __ldcg(skel + (size_t)(cfirst + c) * MAXR + (a - s.coff[c]));
+        }
+        skel[(size_t)t * MAXR + k] = x;
+    }
+    if (tid == 0) g.rank[t] = r;
+    if (!LEAVES) {
+        __syncthreads();
         if (tid == 0) dep_publish(dp, t);
+    }
+    // U = R12 times R11^-1 for the open rows (back substitution, one thread per row), the
+    // pivot rows rows of the identity
+    for (int a = tid; a < m; a += THREADS) {
+        float *u = s.C + a * CS;
+        const int sp = s.selpos[a];
+        if (sp >= 0) {
+            for (int i = 0; i < r; i++) u[i] = i == sp ? 1.f : 0.f;
+        } else {
+            for (int k = r - 1; k >= 0; k--) {
+                const float *col = s.R11 + k * (k + 1) / 2;
+                const float uk = u[k] / col[k];
+                u[k] = uk;
+                for (int i = 0; i < k; i++) u[i] = fmaf(-col[i], uk, u[i]);
+            }
+        }
+    }
+    if (!LEAVES && tid < nch && !tv.leaf[cfirst + tid]) dep_wait_y0(dp, cfirst + tid);
+    __syncthreads();
+    for (int idx = tid; idx < m * r; idx += THREADS) {
+        const int a = idx / r, k = idx - a * r;
+        U[(size_t)a * MAXR + k] = s.C[a * CS + k];
+    }
+    // upward coefficients y0 = U^T (the leaf's [1 | x] | the children's y0): groups of RG
+    // threads over k and THREADS / RG groups over the rows, summed in a fixed order
+    {
+        float4 *part = reinterpret_cast<float4 *>(s.Q);
+        const int RG = r <= 16 ? 16 : (r <= 32 ? 32 : 64);
+        const int C = THREADS / RG, kk = tid % RG, cg = tid / RG;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (kk < r) {
+            for (int a = cg; a < m; a += C) {
+                const float w = s.C[a * CS + kk];
+                if (LEAVES) {
+                    const float4 x = xt[s0 + a];
+                    acc.x += w;
+                    acc.y = fmaf(w, x.x, acc.y);
+                    acc.z = fmaf(w, x.y, acc.z);
+                    acc.w = fmaf(w, x.z, acc.w);
+                } else {
+                    int c = 0;
+                    while (a >= s.coff[c + 1]) c++;
+                    fma4(acc, w, __ldcg(g.y0 + (size_t)(cfirst + c) * MAXR + (a - s.coff[c])));
+                }
+            }
+        }
+        part[tid] = acc;
+        __syncthreads();
+        if (tid < r) {
+            float4 y = part[tid];
+            for (int c = 1; c < C; c++) add4(y, part[c * RG + tid]);
+            g.y0[(size_t)t * MAXR + tid] = y;
+        }
+    }
+    if (!LEAVES) {
+        __syncthreads();
+        if (tid == 0) dep_publish_y0(dp, t);
     }
 }
 
@@ -1553,7 +2021,21 @@ __device__ __forceinline__ void acc_cols(float4 &acc, float w, const float4 &v)
     if (NC == 4) acc.w = fmaf(w, v.w, acc.w);
 }
 
-template <int D, int NC>
+// Parts of the leaf targets' sums: NEAR_ALL = the near blocks and the far entries whose source
+// is finer than the leaf (through the source's skeleton and upward coefficients), assigned;
+// NEAR_BLOCKS = the near blocks alone (tree, points and lists only: no basis), assigned;
+// NEAR_FINE = the finer far entries alone, added.
+constexpr int NEAR_ALL = 0, NEAR_BLOCKS = 1, NEAR_FINE = 2;
+
+// whether leaf t has a far entry whose source is finer (every thread computes the same)
+__device__ __forceinline__ bool has_fine_far(const ProdArgs &g, int t, int lt)
+{
+    for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++)
+        if (g.tv.level[g.far_idx[e]] > lt) return true;
+    return false;
+}
+
+template <int D, int NC, int PART = NEAR_ALL>
 __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
 {
     constexpr int MAXR = Dim<D>::MAXR;
@@ -1566,12 +2048,13 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
     __shared__ float4 sxin[NEAR_THREADS];
     __shared__ float4 sy[MAXR];
     const int s0 = tv.start[t], cnt = tv.end[t] - s0, lt = tv.level[t];
+    if (PART == NEAR_FINE && !has_fine_far(g, t, lt)) return;
     for (int chunk = 0; chunk < cnt; chunk += NEAR_THREADS) {
         const int i = s0 + chunk + threadIdx.x;
         const bool valid = chunk + (int)threadIdx.x < cnt;
         const Vec<D> xi = xt[valid ? i : s0];
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int e = g.near_ptr[t]; e < g.near_ptr[t + 1]; e++) {
+        for (int e = g.near_ptr[t]; PART != NEAR_FINE && e < g.near_ptr[t + 1]; e++) {
             const int s = g.near_idx[e];
             const int ss = tv.start[s], sc = tv.end[s] - ss;
             for (int tile = 0; tile < sc; tile += NEAR_THREADS) {
@@ -1595,7 +2078,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
                 }
             }
         }
-        for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++) {
+        for (int e = g.far_ptr[t]; PART != NEAR_BLOCKS && e < g.far_ptr[t + 1]; e++) {
             const int s = g.far_idx[e];
             if (tv.level[s] <= lt) continue;
             const int rs = g.rank[s];
@@ -1607,7 +2090,10 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
             __syncthreads();
             for (int b = 0; b < rs; b++) acc_cols<NC>(acc, rkernel(dist2(xi, sx[b])), sy[b]);
         }
-        if (valid) g.yp[i] = acc;
+        if (valid) {
+            if (PART == NEAR_FINE) add4(acc, g.yp[i]);
+            g.yp[i] = acc;
+        }
     }
 }
 
@@ -1620,6 +2106,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near(ProdArgs g)
 constexpr int NEAR2_THREADS = 64;
 constexpr int NEAR2_TILE = 2 * NEAR2_THREADS;
 
+template <int PART = NEAR_ALL>
 __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
 {
     constexpr int MAXR = Dim<2>::MAXR;
@@ -1633,12 +2120,13 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
     __shared__ float2 sw2[MAXR];            // (w2, w2)
     const int tid = threadIdx.x;
     const int s0 = tv.start[t], cnt = tv.end[t] - s0, lt = tv.level[t];
+    if (PART == NEAR_FINE && !has_fine_far(g, t, lt)) return;
     for (int chunk = 0; chunk < cnt; chunk += NEAR2_TILE) {
         const int a0 = chunk + tid, a1 = a0 + NEAR2_THREADS;
         const float2 x0 = xt[s0 + (a0 < cnt ? a0 : 0)], x1 = xt[s0 + (a1 < cnt ? a1 : 0)];
         const F2 ax = f2_pack(x0.x, x1.x), ay = f2_pack(x0.y, x1.y);
         F2 acc0 = f2_pack(0.f, 0.f), accx = acc0, accy = acc0;
-        for (int e = g.near_ptr[t]; e < g.near_ptr[t + 1]; e++) {
+        for (int e = g.near_ptr[t]; PART != NEAR_FINE && e < g.near_ptr[t + 1]; e++) {
             const int s = g.near_idx[e];
             const int ss = tv.start[s], sc = tv.end[s] - ss;
             for (int tile = 0; tile < sc; tile += NEAR2_TILE) {
@@ -1675,7 +2163,7 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
                 }
             }
         }
-        for (int e = g.far_ptr[t]; e < g.far_ptr[t + 1]; e++) {
+        for (int e = g.far_ptr[t]; PART != NEAR_BLOCKS && e < g.far_ptr[t + 1]; e++) {
             const int s = g.far_idx[e];
             if (tv.level[s] <= lt) continue;
             const int rs = g.rank[s];
@@ -1702,8 +2190,13 @@ __global__ void __launch_bounds__(NEAR2_THREADS) k_near2d(ProdArgs g)
         f2_unpack(acc0, c00, c01);
         f2_unpack(accx, cx0, cx1);
         f2_unpack(accy, cy0, cy1);
-        if (a0 < cnt) g.yp[s0 + a0] = make_float4(c00, cx0, cy0, 0.f);
-        if (a1 < cnt) g.yp[s0 + a1] = make_float4(c01, cx1, cy1, 0.f);
+        float4 o0 = make_float4(c00, cx0, cy0, 0.f), o1 = make_float4(c01, cx1, cy1, 0.f);
+        if (PART == NEAR_FINE) {
+            if (a0 < cnt) add4(o0, g.yp[s0 + a0]);
+            if (a1 < cnt) add4(o1, g.yp[s0 + a1]);
+        }
+        if (a0 < cnt) g.yp[s0 + a0] = o0;
+        if (a1 < cnt) g.yp[s0 + a1] = o1;
     }
 }
 
@@ -1825,10 +2318,19 @@ public:
     ~H2Impl() override
     {
         if (counts_ev_) cudaEventDestroy(counts_ev_);
+        if (st2_) {
+            cudaStreamSynchronize(st2_);
+            cudaStreamDestroy(st2_);
+        }
+        if (fork_ev_) cudaEventDestroy(fork_ev_);
+        if (near_ev_) cudaEventDestroy(near_ev_);
     }
 
     H2Impl(int n, cudaStream_t st) : n_(n), st_(st)
     {
+        TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+        TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+        TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&near_ev_, cudaEventDisableTiming));
         keys_in_.exact(n); keys_.exact(n); idx_in_.exact(n); perm_.exact(n); xt_.exact(n);
         yp_.exact(n); s_.exact(n); v_.exact(n);
         bbox_part_.exact((size_t)BBOX_BLOCKS * (2 * D + 1));
@@ -1861,10 +2363,17 @@ public:
                                              (int)id2_smem(ID2_THREADS)));
         TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id2d<false, ID2_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)id2_smem(ID2_THREADS)));
+        if (D == 3) {
+            id3_attr<false, 512, ID3_ROWS>();
+            id3_attr<true, 512, ID3_ROWS>();
+            id3_attr<true, 256, ID3_SMALL>();
+            id3_attr<true, 128, ID3_TINY>();
+        }
     }
 
     int build(const void *Y, int leaf_size, double tol, const std::function<void()> *overlap) override
     {
+        join_near();   // the side stream's near field reads the tree this build rewrites
         leaf_size_ = leaf_size;
         const int L = Dim<D>::L;
         cudaEvent_t t_tree = mark_begin();
@@ -1968,7 +2477,8 @@ public:
         y1_.ensure((size_t)n_node_ * MAXR);
         U_.ensure((size_t)std::max<long long>(hrows_, 1) * MAXR);
         const int mcap = id_mcap();
-        const bool need_glob = stats_.max_leaf > mcap || (1 << D) * MAXR > mcap;
+        const bool id3_path = D == 3 && id3_;   // no stored matrix, except for leaves above ID3_ROWS
+        const bool need_glob = id3_path ? stats_.max_leaf > ID3_ROWS : stats_.max_leaf > mcap || (1 << D) * MAXR > mcap;
         if (need_glob) {
             gA_.ensure((size_t)std::max<long long>(hrows_, 1) * (P + 1));
             gnrm_.ensure(std::max<long long>(hrows_, 1));
@@ -1991,6 +2501,7 @@ public:
                 k_id2d<true, ID2_THREADS><<<hbig_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hbig_, blist_.p, il, dp);
             mark_end(t_bases, 2);
             t_bases = mark_begin();
+            near_fork_point();
             if (hint_ > 0 && id_by_level_) {
                 // one launch per level, deepest first (TSNE_ID_BYLEVEL=1)
                 for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
@@ -2002,9 +2513,12 @@ public:
                 }
             } else if (hint_ > 0) {
                 TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
-                k_id2d<false, ID2_THREADS><<<hint_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hint_, ilist_.p, il, dp);
+                DepArgs d2 = dp;
+                d2.flag2 = flag2_.p;
+                k_id2d<false, ID2_THREADS><<<hint_, ID2_THREADS, id2_smem(ID2_THREADS), st_>>>(hint_, ilist_.p, il, d2);
             }
             launches_ += 2;
+            near_launch_side();
             mark_end(t_bases, 7);
             if (timing_) TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
             sec_end("lists+bases");
@@ -2014,6 +2528,39 @@ public:
             return 0;
         }
         DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
+        if (D == 3 && id3_) {
+            // recomputed-row decompositions: leaves by size (llist: at most ID3_TINY points;
+            // blist: the others, up to ID3_ROWS; larger leaves, only at the depth limit, take
+            // k_id), then the internal nodes in one dependency-ordered launch
+            if (stats_.max_leaf <= ID3_ROWS) {
+                if (hleaf_ > 0) id3_launch<true, 128, ID3_TINY>(hleaf_, llist_.p, 0, il, dp);
+                if (hbig_ > 0) {
+                    id3_launch<true, 256, ID3_SMALL>(hbig_, blist_.p, ID3_TINY, il, dp);
+                    if (stats_.max_leaf > ID3_SMALL) id3_launch<true, 512, ID3_ROWS>(hbig_, blist_.p, ID3_SMALL, il, dp);
+                }
+            } else {
+                k_id<D, true><<<n_node_ - first, IDG_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il, 0,
+                                                                                              nullptr, dp);
+                launches_++;
+            }
+            mark_end(t_bases, 2);
+            t_bases = mark_begin();
+            near_fork_point();
+            if (hint_ > 0) {
+                TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
+                DepArgs d2 = dp;
+                d2.flag2 = flag2_.p;
+                id3_launch<false, 512, ID3_ROWS>(hint_, ilist_.p, 0, il, d2);
+            }
+            near_launch_side();
+            mark_end(t_bases, 7);
+            if (timing_) TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
+            sec_end("lists+bases");
+            built_ = true;
+            y0_from_build_ = true;
+            rank_stats_valid_ = false;
+            return 0;
+        }
         k_id<D, true><<<n_node_ - first, IDG_THREADS, id_smem_bytes<D>(mleaf), st_>>>(MIN_ADM_LEVEL, il, 0, nullptr, dp);
         launches_++;
         mark_end(t_bases, 2);
@@ -2251,6 +2798,8 @@ private:
     struct Mark { cudaEvent_t a, b; int phase; };
     bool timing_ = getenv("TSNE_H2_TIMERS") && atoi(getenv("TSNE_H2_TIMERS")) != 0;
     bool id_by_level_ = getenv("TSNE_ID_BYLEVEL") && atoi(getenv("TSNE_ID_BYLEVEL")) != 0;
+    // 3D bases: recomputed rows (k_id3, default) or rows held in memory (k_id, TSNE_ID3=0)
+    bool id3_ = !(getenv("TSNE_ID3") && atoi(getenv("TSNE_ID3")) == 0);
     std::vector<Mark> marks_;
     double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaEvent_t mark_begin()
@@ -2281,6 +2830,20 @@ private:
         marks_.push_back({a, b, phase});
     }
 
+    template <bool LEAVES, int THREADS, int ROWS>
+    static void id3_attr()
+    {
+        TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_id3<LEAVES, THREADS, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(typename Id3<THREADS, ROWS>::Smem)));
+    }
+    template <bool LEAVES, int THREADS, int ROWS>
+    void id3_launch(int n_item, const int *items, int mlo, const IdArgs &a, const DepArgs &dp)
+    {
+        k_id3<LEAVES, THREADS, ROWS><<<n_item, THREADS, sizeof(typename Id3<THREADS, ROWS>::Smem), st_>>>(
+            n_item, items, mlo, a, dp);
+        launches_++;
+    }
+
     static int id_mcap()
     {
         // shared-memory rows of the ID: every internal node of the 2D tree (4 * MAXR rows)
@@ -2296,6 +2859,8 @@ private:
         bset_.exact(c * (Dim<D>::L + 1));
         flag_.exact(c);
         TSNE_CUDA_CHECK(cudaMemsetAsync(flag_.p, 0, sizeof(int) * c, st_));
+        flag2_.exact(c);
+        TSNE_CUDA_CHECK(cudaMemsetAsync(flag2_.p, 0, sizeof(int) * c, st_));
         nid_.exact(c * (Dim<D>::L + 1));
         alloc_lists();
     }
@@ -2359,13 +2924,49 @@ private:
         TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(cub_tmp_.p, bytes, in, out + 1, count, st_));
     }
 
-    void run_product(const float4 *xin = nullptr)
+    ProdArgs prod_args(const float4 *xin)
     {
         ProdArgs g;
         g.xin = xin;
         g.tv = view(); g.xt = xt_.p; g.skel = skel_.p; g.rank = rank_.p; g.rowoff = rowoff_.p; g.U = U_.p;
         g.y0 = y0_.p; g.y1 = y1_.p; g.yp = yp_.p;
         g.far_ptr = far_ptr_.p; g.far_idx = far_idx_.p; g.near_ptr = near_ptr_.p; g.near_idx = near_idx_.p;
+        return g;
+    }
+    template <int PART>
+    void launch_near(const ProdArgs &g, cudaStream_t st)
+    {
+        if (D == 2 && g.xin == nullptr) k_near2d<PART><<<n_node_, NEAR2_THREADS, 0, st>>>(g);
+        else k_near<D, 4, PART><<<n_node_, NEAR_THREADS, 0, st>>>(g);
+        launches_++;
+    }
+    // The near blocks of the force product ([1 | Y] columns) need only the tree, the points and
+    // the near lists, so a build runs them on a side stream beside the internal bases, whose
+    // dependency chain leaves SMs idle. The fork point follows the leaf bases (which fill the
+    // GPU by themselves); the internal bases are queued before the near blocks, so their CTAs
+    // are dispatched first. The product joins the side stream before the first kernel that
+    // adds to their output (the leaves' far entries with finer sources, which read the bases,
+    // then k_down_leaves).
+    void near_fork_point() { TSNE_CUDA_CHECK(cudaEventRecord(fork_ev_, st_)); }
+    void near_launch_side()
+    {
+        TSNE_CUDA_CHECK(cudaStreamWaitEvent(st2_, fork_ev_, 0));
+        launch_near<NEAR_BLOCKS>(prod_args(nullptr), st2_);
+        TSNE_CUDA_CHECK(cudaEventRecord(near_ev_, st2_));
+        near_pending_ = true;
+    }
+    void join_near()
+    {
+        if (!near_pending_) return;
+        TSNE_CUDA_CHECK(cudaStreamWaitEvent(st_, near_ev_, 0));
+        near_pending_ = false;
+    }
+
+    void run_product(const float4 *xin = nullptr)
+    {
+        const bool near_done = near_pending_ && xin == nullptr;   // the side stream's near field
+        if (!near_done) join_near();                              // other columns rewrite it
+        const ProdArgs g = prod_args(xin);
         const TreeInfo &I = *hinfo_.p;
         if (xin != nullptr || !y0_from_build_) {
             for (int l = max_level_; l >= MIN_ADM_LEVEL; l--) {
@@ -2378,17 +2979,20 @@ private:
         cudaEvent_t t_far = mark_begin();
         k_far_c<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(first, n_node_, g);
         mark_end(t_far, 3);
+        launches_++;
         cudaEvent_t t_near = mark_begin();
-        if (D == 2 && xin == nullptr) k_near2d<<<n_node_, NEAR2_THREADS, 0, st_>>>(g);
-        else k_near<D, 4><<<n_node_, NEAR_THREADS, 0, st_>>>(g);
+        if (!near_done) launch_near<NEAR_ALL>(g, st_);
         mark_end(t_near, 4);
-        launches_ += 2;
         cudaEvent_t t_down = mark_begin();
         if (hint_ > 0) {
             TSNE_CUDA_CHECK(cudaMemsetAsync(ticket_.p, 0, sizeof(int), st_));
             DepArgs dp{flag_.p, ticket_.p, &info_.p->pad[1], ++epoch_};
             k_down_internal<D><<<grid_for((long long)hint_ * 32, 256, 148 * 8), 256, 0, st_>>>(hint_, ilist_.p, g, dp);
             launches_++;
+        }
+        if (near_done) {
+            join_near();
+            launch_near<NEAR_FINE>(g, st_);
         }
         k_down_leaves<D><<<grid_for((long long)(n_node_ - first) * 32, 256), 256, 0, st_>>>(g);
         launches_++;
@@ -2420,6 +3024,10 @@ private:
     DevBuf<signed char> delta_;
     DevBuf<int> fm_, blkcnt_, blkoff_, bset_, nid_, btot_;
     DevBuf<int> flag_, ticket_;   // dependency-ordered launches
+    DevBuf<int> flag2_;           // second flags (bases: upward coefficients final)
+    cudaStream_t st2_ = nullptr;  // side stream: the near field beside the internal bases
+    cudaEvent_t fork_ev_ = nullptr, near_ev_ = nullptr;
+    bool near_pending_ = false;
     DevBuf<int> far_slot_, near_slot_;   // 2D: list entries parked by the count pass
     int epoch_ = 0;
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;

@@ -912,15 +912,25 @@ tsne_workspace *create_workspace(int n_point, int pt_dim, int low_dim, const tsn
         ws->klpart.exact(ROW_GRID);
         const bool tm = env_int("TSNE_E2E_TIMERS", 0) != 0;
         double t0 = wall_sec();
+        // the initial embedding (host only) is drawn on another thread while P goes up; the
+        // guard joins it on every way out of this block
+        std::vector<double> Y0((size_t)n_point * low_dim);
+        std::thread init_th([&Y0, n_point, low_dim, params] {
+            initialize_embedding(Y0.data(), n_point, low_dim, params->init_method, params->init_Y,
+                                 (unsigned int)params->random_seed);
+        });
+        struct Joiner {
+            std::thread &t;
+            ~Joiner() { if (t.joinable()) t.join(); }
+        } joiner{init_th};
         if (!load_P(ws)) {
+            init_th.join();
             tsne_destroy(ws);
             return nullptr;
         }
         if (tm) printf("E2E init: P on the device %.1f ms\n", 1e3 * (wall_sec() - t0));
         t0 = wall_sec();
-        std::vector<double> Y0((size_t)n_point * low_dim);
-        initialize_embedding(Y0.data(), n_point, low_dim, params->init_method, params->init_Y,
-                             (unsigned int)params->random_seed);
+        init_th.join();
         ws->params.init_Y = nullptr;
         upload_soa(ws, Y0.data(), ws->Y.p);
         ws->iter_times.assign(std::max(params->n_iter, 0), 0.0);

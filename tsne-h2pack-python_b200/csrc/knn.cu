@@ -11,6 +11,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
+#include <thread>
+#include <chrono>
 #include <climits>
 #include <utility>
 #include <vector>
@@ -267,6 +270,8 @@ k_knn_tiled(int n, int dp, int k, const float *__restrict__ X, const float *__re
 
 namespace tsne {
 
+int knn_tc_run(const float *dX, int n, int dp, int dim, int k, float maxabs, int *dI, float *dD, cudaStream_t st);
+
 // k-NN graph of the n x dim float rows of X (host, row-major) on the device: indices and
 // distances (n x k each, host), rows sorted by index. 0 ok, -1 bad arguments.
 int knn_graph_device(const float *X, int n, int dim, int k, int *idx_out, float *dist_out)
@@ -277,42 +282,83 @@ int knn_graph_device(const float *X, int n, int dim, int k, int *idx_out, float 
     const bool tiled = k <= KNN_MAX_K && smem <= 227 * 1024;
     cudaStream_t st;
     TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    bool failed = false;
+    const bool tm = getenv("TSNE_KNN_TIMERS") && atoi(getenv("TSNE_KNN_TIMERS")) != 0;
+    auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    double t0 = now();
     {
         AllocStream guard(st);
         // centred (distances unchanged; the norms, and so the cancellation in
         // |q|^2 + |p|^2 - 2 q.p, shrink)
+        // on host threads over a fixed partition of the rows (the column sums of each part are
+        // added in part order, so the mean does not depend on the number of threads)
+        constexpr int PARTS = 16;
+        const int nth = std::max(1, std::min(PARTS, (int)std::thread::hardware_concurrency()));
+        auto run_parts = [&](const std::function<void(int)> &fn) {
+            std::vector<std::thread> th;
+            for (int t = 1; t < nth; t++)
+                th.emplace_back([&, t] { for (int part = t; part < PARTS; part += nth) fn(part); });
+            for (int part = 0; part < PARTS; part += nth) fn(part);
+            for (auto &x : th) x.join();
+        };
+        std::vector<double> psum((size_t)PARTS * dim, 0.0);
+        run_parts([&](int part) {
+            const int i0 = (int)((long long)n * part / PARTS), i1 = (int)((long long)n * (part + 1) / PARTS);
+            double *ps = psum.data() + (size_t)part * dim;
+            for (int i = i0; i < i1; i++)
+                for (int c = 0; c < dim; c++) ps[c] += X[(size_t)i * dim + c];
+        });
         std::vector<double> mean(dim, 0.0);
-        for (int i = 0; i < n; i++)
-            for (int c = 0; c < dim; c++) mean[c] += X[(size_t)i * dim + c];
+        for (int part = 0; part < PARTS; part++)
+            for (int c = 0; c < dim; c++) mean[c] += psum[(size_t)part * dim + c];
         for (int c = 0; c < dim; c++) mean[c] /= n;
-        std::vector<float> Xp((size_t)n * dp, 0.f), nrm(n);
-        for (int i = 0; i < n; i++) {
-            float s2 = 0.f;
-            for (int c = 0; c < dim; c++) {
-                const float v = (float)((double)X[(size_t)i * dim + c] - mean[c]);
-                Xp[(size_t)i * dp + c] = v;
-                s2 = fmaf(v, v, s2);
+        std::vector<float> Xp((size_t)n * dp, 0.f), nrm(n), pmax(PARTS, 0.f);
+        run_parts([&](int part) {
+            const int i0 = (int)((long long)n * part / PARTS), i1 = (int)((long long)n * (part + 1) / PARTS);
+            float mx = 0.f;
+            for (int i = i0; i < i1; i++) {
+                float s2 = 0.f;
+                for (int c = 0; c < dim; c++) {
+                    const float v = (float)((double)X[(size_t)i * dim + c] - mean[c]);
+                    Xp[(size_t)i * dp + c] = v;
+                    s2 = fmaf(v, v, s2);
+                    mx = std::max(mx, std::fabs(v));
+                }
+                nrm[i] = s2;
             }
-            nrm[i] = s2;
-        }
+            pmax[part] = mx;
+        });
+        const float maxabs = *std::max_element(pmax.begin(), pmax.end());
+        if (tm) printf("KNN host centring %.1f ms\n", 1e3 * (now() - t0));
+        t0 = now();
         DevBuf<float> dX, dN, dD;
         DevBuf<int> dI;
         dX.exact(Xp.size()); dN.exact(n); dD.exact((size_t)n * k); dI.exact((size_t)n * k);
         TSNE_CUDA_CHECK(cudaMemcpyAsync(dX.p, Xp.data(), sizeof(float) * Xp.size(), cudaMemcpyHostToDevice, st));
         TSNE_CUDA_CHECK(cudaMemcpyAsync(dN.p, nrm.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
-        if (tiled) {
+        // the tensor-core scan where it applies (k <= 128, at most 64 dimensions), else the
+        // CUDA-core one
+        if (tm) { cudaStreamSynchronize(st); printf("KNN upload %.1f ms\n", 1e3 * (now() - t0)); t0 = now(); }
+        const int tc = tiled ? knn_tc_run(dX.p, n, dp, dim, k, maxabs, dI.p, dD.p, st) : 1;
+        failed = tc < 0;
+        if (tc == 1 && tiled) {
             TSNE_CUDA_CHECK(cudaFuncSetAttribute(k_knn_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_knn_tiled<<<(n + KQ - 1) / KQ, KNN_THREADS, smem, st>>>(n, dp, k, dX.p, dN.p, dI.p, dD.p);
-        } else {
+        } else if (tc == 1) {
             // squared distances sorted by (distance, index); re-sorted by index on the host below
             k_knn_warp<<<std::min((n + 3) / 4, 148 * 32), 128, 0, st>>>(n, dp, dX.p, k, dI.p, dD.p);
         }
         TSNE_CUDA_CHECK(cudaGetLastError());
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(idx_out, dI.p, sizeof(int) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
-        TSNE_CUDA_CHECK(cudaMemcpyAsync(dist_out, dD.p, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+        if (tm) { cudaStreamSynchronize(st); printf("KNN scan %.1f ms\n", 1e3 * (now() - t0)); t0 = now(); }
+        if (!failed) {
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(idx_out, dI.p, sizeof(int) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+            TSNE_CUDA_CHECK(cudaMemcpyAsync(dist_out, dD.p, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+        }
         TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
     }
     cudaStreamDestroy(st);
+    if (tm) printf("KNN download %.1f ms\n", 1e3 * (now() - t0));
+    if (failed) return -1;
     if (!tiled) {
         std::vector<std::pair<int, float>> row(k);
         for (int i = 0; i < n; i++) {

@@ -16,7 +16,8 @@
 // tile's 128 dot products, form the distances and keep the row's best k in a max-heap ordered
 // by (distance, index), as k_knn_tiled's selection keeps them (ties: the smaller index). The
 // stages and accumulators are handed over with mbarriers; every wait is bounded (about two
-// seconds), after which the kernel records an error the host reports. The output rows are
+// seconds), after which the kernel records an error the host reports, and once one wait of the
+// launch has given up every other wait returns at once. The output rows are
 // sorted by index and the reported distances recomputed from the FP32 coordinates' differences.
 #include <cuda_fp16.h>
 #include <math.h>
@@ -71,8 +72,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// wait for the phase of parity `parity` to complete; false when the bound ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+// wait for the phase of parity `parity` to complete; false when the bound ran out (the wait
+// then sets *err) or when another wait of the launch already gave up (so that a launch that
+// fails stops within about one bound, not one bound per wait)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err)
 {
     const unsigned long long t0 = global_ns();
     for (;;) {
@@ -85,7 +88,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
             : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
-        if (global_ns() - t0 > TC_WAIT_NS) return false;
+        if (*reinterpret_cast<volatile int *>(err) != 0) return false;
+        if (global_ns() - t0 > TC_WAIT_NS) {
+            atomicExch(err, 1);
+            return false;
+        }
     }
 }
 // global -> shared bulk copy completing on an mbarrier (16-byte aligned, multiple of 16 bytes)
@@ -201,7 +208,7 @@ struct TcBars {
 // wait for u's stage and for the epilogue to have released u's accumulator (tile u - 2), issue
 // the 12 MMAs, commit to the accumulator's and the stage's barriers
 __device__ bool tc_producer(const unsigned char *blocks, int qt, int ntile, uint32_t sA, uint32_t sB, uint32_t tmem,
-                            const TcBars &b)
+                            const TcBars &b, int *err)
 {
     bool ok = true;
     mbar_expect_tx(b.a, TC_BLOCK);
@@ -212,15 +219,15 @@ __device__ bool tc_producer(const unsigned char *blocks, int qt, int ntile, uint
         bulk_copy(sB + s * TC_BLOCK, blocks + (size_t)((qt + u) % ntile) * TC_BLOCK, TC_BLOCK, b.full[s]);
     };
     load(0);
-    ok &= mbar_wait(b.a, 0);
+    ok &= mbar_wait(b.a, 0, err);
     for (int u = 0; u < ntile; u++) {
         if (u + 1 < ntile) {
-            if (u + 1 >= 2) ok &= mbar_wait(b.empty[(u + 1) & 1], (((u + 1) >> 1) - 1) & 1);
+            if (u + 1 >= 2) ok &= mbar_wait(b.empty[(u + 1) & 1], (((u + 1) >> 1) - 1) & 1, err);
             load(u + 1);
         }
         const int s = u & 1;
-        ok &= mbar_wait(b.full[s], (u >> 1) & 1);
-        if (u >= 2) ok &= mbar_wait(b.acc_empty[s], ((u >> 1) - 1) & 1);
+        ok &= mbar_wait(b.full[s], (u >> 1) & 1, err);
+        if (u >= 2) ok &= mbar_wait(b.acc_empty[s], ((u >> 1) - 1) & 1, err);
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(s * TC_N);
         const uint32_t bs = sB + s * TC_BLOCK;
@@ -234,13 +241,13 @@ __device__ bool tc_producer(const unsigned char *blocks, int qt, int ntile, uint
         tc_commit(b.empty[s]);
     }
     // the last commits: every MMA has finished before the CTA frees tensor memory
-    if (ntile >= 1) ok &= mbar_wait(b.empty[(ntile - 1) & 1], ((ntile - 1) >> 1) & 1);
+    if (ntile >= 1) ok &= mbar_wait(b.empty[(ntile - 1) & 1], ((ntile - 1) >> 1) & 1, err);
     return ok;
 }
 
 // max-heap of the row's best kh candidates (root: the worst, by (distance, index)) in shared
 // memory, position e of row r at e * TC_M + r; replace the root with (d, p) and sift down
-__device__ __noinline__ void heap_replace(float *hd, int *hx, int kh, int r, float d, int p)
+__device__ __forceinline__ void heap_sift(float *hd, int *hx, int kh, int r, float d, int p)
 {
     int pos = 0;
     for (;;) {
@@ -261,6 +268,10 @@ __device__ __noinline__ void heap_replace(float *hd, int *hx, int kh, int r, flo
     hd[pos * TC_M + r] = d;
     hx[pos * TC_M + r] = p;
 }
+__device__ __noinline__ void heap_replace(float *hd, int *hx, int kh, int r, float d, int p)
+{
+    heap_sift(hd, hx, kh, r, d, p);
+}
 
 // warps 0-3: thread r = query q0 + r = tensor-memory lane r. Per tile: the tile's norms (thread
 // r loads column r's, one tile ahead, exchanged through shared memory), the 128 dot products in
@@ -268,7 +279,7 @@ __device__ __noinline__ void heap_replace(float *hd, int *hx, int kh, int r, flo
 // distances and their minimum; only when the minimum reaches the row's threshold are the
 // candidates tested one by one
 __device__ bool tc_epilogue(int n, int kh, int qt, int ntile, const unsigned char *blocks, const float *qnorm,
-                            uint32_t tmem, const TcBars &b, float *hd, int *hx, float *nbuf)
+                            uint32_t tmem, const TcBars &b, float *hd, int *hx, float *nbuf, int *err)
 {
     bool ok = true;
     const int r = threadIdx.x, wid = r >> 5;
@@ -278,7 +289,7 @@ __device__ bool tc_epilogue(int n, int kh, int qt, int ntile, const unsigned cha
         const int ti = (qt + u) % ntile;
         return __ldg(reinterpret_cast<const float *>(blocks + (size_t)ti * TC_BLOCK + 2 * TC_HALF_BYTES) + r);
     };
-    ok &= mbar_wait(b.a, 0);
+    ok &= mbar_wait(b.a, 0, err);
     const float qn = qnorm[r];
     float tau = INFINITY;
     int taui = INT_MAX;
@@ -289,7 +300,7 @@ __device__ bool tc_epilogue(int n, int kh, int qt, int ntile, const unsigned cha
         nbuf[s * TC_N + r] = pn_next;
         if (u + 1 < ntile) pn_next = norm_at(u + 1);
         asm volatile("bar.sync 1, %0;" ::"n"(TC_M) : "memory");
-        ok &= mbar_wait(b.acc_full[s], (u >> 1) & 1);
+        ok &= mbar_wait(b.acc_full[s], (u >> 1) & 1, err);
         tc_fence_after();
         uint32_t v[TC_N];
         tmem_ld128(tmem + ((uint32_t)(wid * 32) << 16) + (uint32_t)(s * TC_N), v);
@@ -376,10 +387,10 @@ k_knn_tc(int n, int dp, int k, int kh, int ntile, const unsigned char *__restric
     const uint32_t tmem = *holder;
     bool ok = true;
     if (wid == 4) {
-        if (lane == 0) ok = tc_producer(blocks, qt, ntile, smem_u32(sA), smem_u32(sB), tmem, b);
+        if (lane == 0) ok = tc_producer(blocks, qt, ntile, smem_u32(sA), smem_u32(sB), tmem, b, err);
     } else {
         ok = tc_epilogue(n, kh, qt, ntile, blocks, reinterpret_cast<const float *>(sA + 2 * TC_HALF_BYTES), tmem, b,
-                         hd, hx, nbuf);
+                         hd, hx, nbuf, err);
     }
     if (!ok) atomicExch(err, 1);
     tc_fence_before();

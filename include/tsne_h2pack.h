@@ -154,8 +154,12 @@ TSNE_API tsne_workspace_t *tsne_init_with_knn_distances(const DTYPE *X, int n_po
  * (tsne_h2pack/_knn_methods.py:71-119, knn_method='exact'; no counterpart entry point in its C
  * ABI). indices and distances (host, n_samples x k each) receive each row's k neighbours
  * sorted by index, self excluded, distances not squared (single precision; ties of distance
- * keep the smaller index). 1 <= k <= min(n_samples - 1, 256), n_samples <= 2^24. Returns 0,
- * -1 on bad arguments, -2 on a device error. */
+ * keep the smaller index). With at most 64 features and k <= 128 the distances come from the
+ * tensor cores (FP16 high and low parts of the centred coordinates, FP32 accumulation) and the
+ * best k + 16 of each row are re-ranked by exact FP32 distances; otherwise from an FP32 scan on
+ * the CUDA cores. 1 <= k <= min(n_samples - 1, 256), n_samples <= 2^24. Returns 0, -1 on bad
+ * arguments, -2 on a device error (a bounded wait of the tensor-core scan that gave up
+ * included). */
 TSNE_API int tsne_knn_graph(const float *X, int n_samples, int n_features, int k, int *indices, float *distances);
 
 /* init='pca' on the device (reference tsne_h2pack/manifold.py:399-416, there scikit-learn's

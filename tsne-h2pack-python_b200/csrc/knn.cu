@@ -273,7 +273,8 @@ namespace tsne {
 int knn_tc_run(const float *dX, int n, int dp, int dim, int k, float maxabs, int *dI, float *dD, cudaStream_t st);
 
 // k-NN graph of the n x dim float rows of X (host, row-major) on the device: indices and
-// distances (n x k each, host), rows sorted by index. 0 ok, -1 bad arguments.
+// distances (n x k each, host), rows sorted by index. 0 ok, -1 bad arguments, -2 a bounded wait
+// of the tensor-core scan gave up.
 int knn_graph_device(const float *X, int n, int dim, int k, int *idx_out, float *dist_out)
 {
     if (X == nullptr || n < 2 || dim < 1 || k < 1 || k > n - 1 || k > KNN_WARP_MAX_K || n > (1 << 24)) return -1;
@@ -358,7 +359,7 @@ int knn_graph_device(const float *X, int n, int dim, int k, int *idx_out, float 
     }
     cudaStreamDestroy(st);
     if (tm) printf("KNN download %.1f ms\n", 1e3 * (now() - t0));
-    if (failed) return -1;
+    if (failed) return -2;
     if (!tiled) {
         std::vector<std::pair<int, float>> row(k);
         for (int i = 0; i < n; i++) {

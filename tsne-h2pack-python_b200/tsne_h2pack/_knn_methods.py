@@ -33,7 +33,8 @@ class ExactKNN(_KNN):
 
 
 class CudaKNN(_KNN):
-    """The exact graph on the device (tsne_knn_graph: tiled FP32 scan, rows sorted by index);
+    """The exact graph on the device (tsne_knn_graph: tensor-core distance tiles, candidates
+    re-ranked by exact FP32 distances; the CUDA-core scan above 64 dimensions; rows sorted by index);
     the same neighbours as 'exact' except where two distances tie to single precision."""
     name = "cuda"
 

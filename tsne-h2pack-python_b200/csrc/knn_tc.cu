@@ -273,11 +273,27 @@ __device__ __noinline__ void heap_replace(float *hd, int *hx, int kh, int r, flo
     heap_sift(hd, hx, kh, r, d, p);
 }
 
+// element b (a runtime index below 32) of the registers v[base .. base + 31]: a tree of selects,
+// so the array stays in registers
+template <int N>
+__device__ __forceinline__ float pick32(const uint32_t (&v)[N], int base, int b)
+{
+    float x[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) x[i] = __uint_as_float((b & 16) ? v[base + 16 + i] : v[base + i]);
+#pragma unroll
+    for (int w = 8; w >= 1; w >>= 1) {
+#pragma unroll
+        for (int i = 0; i < w; i++) x[i] = (b & w) ? x[w + i] : x[i];
+    }
+    return x[0];
+}
+
 // warps 0-3: thread r = query q0 + r = tensor-memory lane r. Per tile: the tile's norms (thread
 // r loads column r's, one tile ahead, exchanged through shared memory), the 128 dot products in
 // one tensor-memory load (the accumulator is released as soon as they are in registers), the
-// distances and their minimum; only when the minimum reaches the row's threshold are the
-// candidates tested one by one
+// distances and their minimum per 32-column chunk; in a chunk whose minimum reaches the row's
+// threshold the candidates form a bit mask, and only its set bits are tested again and inserted
 __device__ bool tc_epilogue(int n, int kh, int qt, int ntile, const unsigned char *blocks, const float *qnorm,
                             uint32_t tmem, const TcBars &b, float *hd, int *hx, float *nbuf, int *err)
 {
@@ -307,20 +323,32 @@ __device__ bool tc_epilogue(int n, int kh, int qt, int ntile, const unsigned cha
         tc_fence_before();
         mbar_arrive(b.acc_empty[s]);
         const float *nb = nbuf + s * TC_N;
-        float m4[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+        float cmin[TC_N / 32] = {INFINITY, INFINITY, INFINITY, INFINITY};   // per 32-column chunk
 #pragma unroll
         for (int j = 0; j < TC_N; j++) {
             const float d = fmaxf(fmaf(-2.f, __uint_as_float(v[j]), qn + nb[j]), 0.f);
             v[j] = __float_as_uint(d);
-            m4[j & 3] = fminf(m4[j & 3], d);
+            cmin[j >> 5] = fminf(cmin[j >> 5], d);
         }
-        const float dmin = fminf(fminf(m4[0], m4[1]), fminf(m4[2], m4[3]));
-        if (live && dmin <= tau) {
+        if (!live) continue;
 #pragma unroll
-            for (int j = 0; j < TC_N; j++) {
-                const float d = __uint_as_float(v[j]);
-                const int p = p0 + j;
-                if ((d < tau || (d == tau && p < taui)) && p < n && p != q) {
+        for (int c = 0; c < TC_N / 32; c++) {
+            if (!(cmin[c] <= tau)) continue;
+            // the chunk's candidates as a bit mask (no branches), then only its set bits
+            uint32_t mask = 0;
+#pragma unroll
+            for (int b = 0; b < 32; b++) {
+                const float d = __uint_as_float(v[32 * c + b]);
+                const int p = p0 + 32 * c + b;
+                const bool pass = (d < tau || (d == tau && p < taui)) && p < n && p != q;
+                mask |= (uint32_t)pass << b;
+            }
+            while (mask != 0) {
+                const int b = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const float d = pick32(v, 32 * c, b);
+                const int p = p0 + 32 * c + b;
+                if (d < tau || (d == tau && p < taui)) {
                     heap_replace(hd, hx, kh, r, d, p);
                     tau = hd[r];
                     taui = hx[r];

@@ -723,7 +723,8 @@ inline int ew_grid(int n) { int g = ceil_div(n, EW_BLOCK); return g < 1 ? 1 : (g
 // per thread, so twice the resident warps). A form is taken
 // while the average CTA's row range fits in half its window; all three modes and the
 // centring follow the same rule, so a step's kernels always agree on the row split. 0 (the
-// default): k_attr_update.
+// default): k_attr_update. Measured at 1M points, 2D: form 2 takes 1.40 ms per launch, form 1
+// 0.651 ms, k_attr_update 0.62 ms.
 template <int D>
 int window_form(int n)
 {

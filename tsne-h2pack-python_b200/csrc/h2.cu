@@ -2324,6 +2324,7 @@ public:
         }
         if (fork_ev_) cudaEventDestroy(fork_ev_);
         if (near_ev_) cudaEventDestroy(near_ev_);
+        if (lists_ev_) cudaEventDestroy(lists_ev_);
     }
 
     H2Impl(int n, cudaStream_t st) : n_(n), st_(st)
@@ -2331,6 +2332,7 @@ public:
         TSNE_CUDA_CHECK(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
         TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
         TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&near_ev_, cudaEventDisableTiming));
+        TSNE_CUDA_CHECK(cudaEventCreateWithFlags(&lists_ev_, cudaEventDisableTiming));
         keys_in_.exact(n); keys_.exact(n); idx_in_.exact(n); perm_.exact(n); xt_.exact(n);
         yp_.exact(n); s_.exact(n); v_.exact(n);
         bbox_part_.exact((size_t)BBOX_BLOCKS * (2 * D + 1));
@@ -2447,25 +2449,38 @@ public:
         stats_.max_leaf = I.max_leaf;
         if (max_level_ <= 2) { built_ = false; return 1; }
 
-        cudaEvent_t t_lists = mark_begin();
+        // The list write (and in 3D the segmented sort of each target's entries) needs only the
+        // count pass, and the bases read no list, so it runs on the side stream beside the leaf
+        // bases; the near blocks follow it there. Its buffers are allocated first, in the
+        // workspace stream's order (the stream-ordered pool), and the side stream starts from
+        // that point. Readers on the workspace stream join it first (join_lists).
         stats_.n_far = htot_[0];
         stats_.n_near = htot_[1];
         far_idx_.ensure(std::max(1, htot_[0]));
         near_idx_.ensure(std::max(1, htot_[1]));
+        if (D == 3) {
+            sort_reserve(far_idx_, far_alt_, htot_[0], far_ptr_.p);
+            sort_reserve(near_idx_, near_alt_, htot_[1], near_ptr_.p);
+        }
         {
+            TSNE_CUDA_CHECK(cudaEventRecord(fork_ev_, st_));
+            TSNE_CUDA_CHECK(cudaStreamWaitEvent(st2_, fork_ev_, 0));
+            cudaEvent_t t_lists = mark_begin(st2_);
             ListOut lo = list_out(1);
             if (D == 2 && !I.pad[2]) {
-                k_lists_compact<<<grid_for((long long)n_node_ * 32, 256, 148 * 8), 256, 0, st_>>>(view(), lo);
+                k_lists_compact<<<grid_for((long long)n_node_ * 32, 256, 148 * 8), 256, 0, st2_>>>(view(), lo);
             } else {
-                k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st_>>>(n_node_, view(), lo);
+                k_lists_write<D><<<grid_for(n_node_, 128, 148 * 8), 128, 0, st2_>>>(n_node_, view(), lo);
             }
             launches_++;
             if (D == 3) {
-                sort_segments(far_idx_, far_alt_, htot_[0], far_ptr_.p);
-                sort_segments(near_idx_, near_alt_, htot_[1], near_ptr_.p);
+                sort_segments(far_idx_, far_alt_, htot_[0], far_ptr_.p, st2_);
+                sort_segments(near_idx_, near_alt_, htot_[1], near_ptr_.p, st2_);
             }
+            mark_end(t_lists, 1, st2_);
+            TSNE_CUDA_CHECK(cudaEventRecord(lists_ev_, st2_));
+            lists_pending_ = true;
         }
-        mark_end(t_lists, 1);
 
         // bases, bottom-up
         cudaEvent_t t_bases = mark_begin();
@@ -2715,6 +2730,7 @@ public:
 
     void copy_lists(int *far_ptr, int *far_idx, int *near_ptr, int *near_idx) override
     {
+        join_lists();
         TSNE_CUDA_CHECK(cudaStreamSynchronize(st_));
         TSNE_CUDA_CHECK(cudaMemcpy(far_ptr, far_ptr_.p, sizeof(int) * (n_node_ + 1), cudaMemcpyDeviceToHost));
         TSNE_CUDA_CHECK(cudaMemcpy(near_ptr, near_ptr_.p, sizeof(int) * (n_node_ + 1), cudaMemcpyDeviceToHost));
@@ -2802,12 +2818,12 @@ private:
     bool id3_ = !(getenv("TSNE_ID3") && atoi(getenv("TSNE_ID3")) == 0);
     std::vector<Mark> marks_;
     double phase_ms_[N_PHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
-    cudaEvent_t mark_begin()
+    cudaEvent_t mark_begin(cudaStream_t st = nullptr)
     {
         cudaEvent_t e = nullptr;
         if (!timing_) return e;
         TSNE_CUDA_CHECK(cudaEventCreate(&e));
-        TSNE_CUDA_CHECK(cudaEventRecord(e, st_));
+        TSNE_CUDA_CHECK(cudaEventRecord(e, st ? st : st_));
         return e;
     }
     // host wall time of one build section; sections slower than 10 ms are reported
@@ -2821,12 +2837,12 @@ private:
                               n_node_, stats_.max_leaf, htot_[0], htot_[1], nset_cap_, cap_node_);
         sec_t0_ = std::chrono::steady_clock::now();
     }
-    void mark_end(cudaEvent_t a, int phase)
+    void mark_end(cudaEvent_t a, int phase, cudaStream_t st = nullptr)
     {
         if (!timing_) return;
         cudaEvent_t b;
         TSNE_CUDA_CHECK(cudaEventCreate(&b));
-        TSNE_CUDA_CHECK(cudaEventRecord(b, st_));
+        TSNE_CUDA_CHECK(cudaEventRecord(b, st ? st : st_));
         marks_.push_back({a, b, phase});
     }
 
@@ -2900,8 +2916,7 @@ private:
         size_t bytes = cub_tmp_.cap;
         TSNE_CUDA_CHECK(cub::DeviceScan::InclusiveSum(cub_tmp_.p, bytes, in, out + 1, count, st_));
     }
-    // ascending order inside every node's segment [ptr[t], ptr[t + 1]) of idx (count entries)
-    void sort_segments(DevBuf<int> &idx, DevBuf<int> &alt, int count, const int *ptr)
+    void sort_reserve(DevBuf<int> &idx, DevBuf<int> &alt, int count, const int *ptr)
     {
         if (count <= 1) return;
         alt.ensure(count);
@@ -2909,8 +2924,15 @@ private:
         size_t need = 0;
         TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortKeys(nullptr, need, keys, count, n_node_, ptr, ptr + 1, st_));
         if (need > cub_tmp_.cap) cub_tmp_.exact(need + 256);
+    }
+    // ascending order inside every node's segment [ptr[t], ptr[t + 1]) of idx (count entries)
+    // (sort_reserve allocates its partner buffer and scratch beforehand)
+    void sort_segments(DevBuf<int> &idx, DevBuf<int> &alt, int count, const int *ptr, cudaStream_t st)
+    {
+        if (count <= 1) return;
+        cub::DoubleBuffer<int> keys(idx.p, alt.p);
         size_t bytes = cub_tmp_.cap;
-        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortKeys(cub_tmp_.p, bytes, keys, count, n_node_, ptr, ptr + 1, st_));
+        TSNE_CUDA_CHECK(cub::DeviceSegmentedSort::SortKeys(cub_tmp_.p, bytes, keys, count, n_node_, ptr, ptr + 1, st));
         if (keys.Current() != idx.p) idx.swap(alt);
         launches_ += 2;
     }
@@ -2955,8 +2977,15 @@ private:
         TSNE_CUDA_CHECK(cudaEventRecord(near_ev_, st2_));
         near_pending_ = true;
     }
+    void join_lists()
+    {
+        if (!lists_pending_) return;
+        TSNE_CUDA_CHECK(cudaStreamWaitEvent(st_, lists_ev_, 0));
+        lists_pending_ = false;
+    }
     void join_near()
     {
+        join_lists();
         if (!near_pending_) return;
         TSNE_CUDA_CHECK(cudaStreamWaitEvent(st_, near_ev_, 0));
         near_pending_ = false;
@@ -2966,6 +2995,7 @@ private:
     {
         const bool near_done = near_pending_ && xin == nullptr;   // the side stream's near field
         if (!near_done) join_near();                              // other columns rewrite it
+        else join_lists();
         const ProdArgs g = prod_args(xin);
         const TreeInfo &I = *hinfo_.p;
         if (xin != nullptr || !y0_from_build_) {
@@ -3025,9 +3055,9 @@ private:
     DevBuf<int> fm_, blkcnt_, blkoff_, bset_, nid_, btot_;
     DevBuf<int> flag_, ticket_;   // dependency-ordered launches
     DevBuf<int> flag2_;           // second flags (bases: upward coefficients final)
-    cudaStream_t st2_ = nullptr;  // side stream: the near field beside the internal bases
-    cudaEvent_t fork_ev_ = nullptr, near_ev_ = nullptr;
-    bool near_pending_ = false;
+    cudaStream_t st2_ = nullptr;  // side stream: the list write and the near field beside the bases
+    cudaEvent_t fork_ev_ = nullptr, near_ev_ = nullptr, lists_ev_ = nullptr;
+    bool near_pending_ = false, lists_pending_ = false;
     DevBuf<int> far_slot_, near_slot_;   // 2D: list entries parked by the count pass
     int epoch_ = 0;
     DevBuf<int> nset_, nset_cnt_, far_cnt_, near_cnt_, far_ptr_, near_ptr_, far_idx_, near_idx_;

@@ -73,3 +73,38 @@ def test_no_cpu_fallback_without_a_device():
     X, G, P, _ = problem(300, seed=0, k=30, perplexity=10.0, dim=8, n_clusters=3)
     with pytest.raises(RuntimeError):
         TSNE(metric="precomputed", perplexity=10, max_iter=10, init="random").fit_transform(G)
+
+
+def test_prepare_knn_graph_drops_self_entries_and_sorts():
+    """The graph handed to the device calibration: rows sorted by column, self entries dropped,
+    for k-NN graphs (k entries in every row) and ragged graphs alike; a k-NN graph without
+    self entries passes through unchanged."""
+    from scipy.sparse import csr_matrix
+    from tsne_h2pack._backend import TSNEBackend
+    prep = TSNEBackend.prepare_knn_graph
+    rng = np.random.default_rng(3)
+    n, k = 50, 6
+    idx = np.stack([rng.choice(np.delete(np.arange(n), i), k, replace=False) for i in range(n)]).astype(np.int32)
+    dist = rng.random((n, k)) + 0.1
+    G = csr_matrix((dist.ravel(), idx.ravel(), np.arange(0, (n + 1) * k, k)), shape=(n, n))
+    G.sort_indices()
+    assert prep(G) is G
+    # unsorted rows with self entries in rows 3 and 17
+    idx2 = idx.copy()
+    idx2[3, 2], idx2[17, 0] = 3, 17
+    G2 = csr_matrix((dist.ravel(), idx2.ravel(), np.arange(0, (n + 1) * k, k)), shape=(n, n))
+    out = prep(G2)
+    assert out.has_sorted_indices and out.nnz == n * k - 2
+    dense_in, dense_out = G2.toarray(), out.toarray()
+    np.fill_diagonal(dense_in, 0.0)
+    np.testing.assert_array_equal(dense_out, dense_in)
+    # ragged rows: the general path
+    G3 = G2.tolil()
+    G3[5, [c for c in range(n) if G3[5, c] != 0][:2]] = 0
+    G3 = csr_matrix(G3)
+    G3.eliminate_zeros()
+    out3 = prep(G3)
+    d3 = G3.toarray()
+    np.fill_diagonal(d3, 0.0)
+    np.testing.assert_array_equal(out3.toarray(), d3)
+    assert not np.any(out3.indices == np.repeat(np.arange(n), np.diff(out3.indptr)))

@@ -495,6 +495,7 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
     std::vector<StageEv> stages;
 
     int ret = 0;
+    bool z_checked = false;   // the current Z has passed the collapse check
     for (int iter = it_begin; iter < it_end; iter++) {
         const double t_iter = wall_sec();
         const double mom = iter >= p.momentum_switch_iter ? p.momentum : p.initial_momentum;
@@ -569,13 +570,21 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
         }
         if (prof && !reuse) { stage_event(ws, evpool, evused); stages.push_back({iter, 2, e1, evused - 1}); }
 
+        // Z collapse stop (reference tsne_h2pack.c:1853-1861). A reuse iteration's Z is the
+        // stored one, which the product iteration that stored it has checked already (a failed
+        // product sets Z = 1 and stops there), so only the first check after a new Z reads it
+        // back: one host synchronisation per product iteration instead of one per iteration.
+        if (!reuse) z_checked = false;
         if (!sklearn && iter > p.momentum_switch_iter) {
             if (reuse) TSNE_CUDA_CHECK(cudaMemcpyAsync(&ws->sc.p->Z, &ws->sc.p->rep_Z, sizeof(double), cudaMemcpyDeviceToDevice, st));
-            TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
-            TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
-            if (ws->hsc.p->Z < 10.0) {
-                if (verbose) printf("\n*** STOPPING: Z collapsed to %.3e (threshold: 10.0) ***\n", ws->hsc.p->Z);
-                break;
+            if (!z_checked) {
+                TSNE_CUDA_CHECK(cudaMemcpyAsync(ws->hsc.p, ws->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+                TSNE_CUDA_CHECK(cudaStreamSynchronize(st));
+                if (ws->hsc.p->Z < 10.0) {
+                    if (verbose) printf("\n*** STOPPING: Z collapsed to %.3e (threshold: 10.0) ***\n", ws->hsc.p->Z);
+                    break;
+                }
+                z_checked = true;
             }
         }
         const bool want_kl = (verbose && iter % 50 == 0) || iter == n_iter - 1;

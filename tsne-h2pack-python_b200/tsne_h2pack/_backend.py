@@ -322,7 +322,14 @@ class TSNEBackend:
         if not knn_distances_csr.has_sorted_indices:
             knn_distances_csr = knn_distances_csr.copy()
             knn_distances_csr.sort_indices()
-        rows = np.repeat(np.arange(n), np.diff(knn_distances_csr.indptr))
+        lens = np.diff(knn_distances_csr.indptr)
+        if n > 0 and knn_distances_csr.nnz == n * int(lens[0]) and np.all(lens == lens[0]):
+            # k entries in every row (a k-NN graph): compare in place, rows as a broadcast column
+            k = int(lens[0])
+            if k == 0 or not np.any(knn_distances_csr.indices.reshape(n, k) ==
+                                    np.arange(n, dtype=knn_distances_csr.indices.dtype)[:, None]):
+                return knn_distances_csr
+        rows = np.repeat(np.arange(n, dtype=np.int32), lens)
         if np.any(knn_distances_csr.indices == rows):
             keep = knn_distances_csr.indices != rows
             knn_distances_csr = csr_matrix(

@@ -53,17 +53,29 @@ def metric_name(n, iters, d=2):
 def data_desc(n, seed=1):
     return f"synthetic: {n:,} x 50 float32 Zipf(1.1) Gaussian mixture, seed {seed}; exact k=90 graph"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
-# ncu summary of the roofline kernel on a smaller case; its DRAM traffic per algorithmic byte
-# scales the traffic to this workload's launch
-TRAFFIC = ROOT / "profiles" / "k_attr_update_200k_full.md"
+# ncu summaries of the roofline kernel on a smaller case (the default 2D form first); the DRAM
+# traffic per algorithmic byte scales the traffic to this workload's launch
+TRAFFIC = [ROOT / "profiles" / "k_attr_update_pf_200k_full.md", ROOT / "profiles" / "k_attr_update_200k_full.md"]
+
+# the attractive step's form (TSNE_ATTR_PIPE; default 3 in 2D, 1 in 3D), as the engine picks it
+ATTR_FORMS = {0: "k_attr_update", 1: "k_attr_update_pf<1> (next step's entries loaded ahead)",
+              2: "k_attr_pair (two rows per half-warp)", 3: "k_attr_update_pf<2> (next step's columns loaded ahead)"}
+
+
+def attr_form(d):
+    v = os.environ.get("TSNE_ATTR_PIPE", "")
+    if v == "":
+        return 3 if d == 2 else 1
+    return int(v) if v.isdigit() and int(v) in ATTR_FORMS else 0
 
 
 def traffic_ratio():
-    """DRAM bytes (read + write) per algorithmic byte of k_attr_update, from the committed ncu
-    summary (line 'traffic_over_algorithmic: X'), or None."""
-    if not TRAFFIC.exists():
+    """DRAM bytes (read + write) per algorithmic byte of the attractive step, from the first
+    committed ncu summary present (line 'traffic_over_algorithmic: X'), or None."""
+    path = next((p for p in TRAFFIC if p.exists()), None)
+    if path is None:
         return None
-    for line in TRAFFIC.read_text().splitlines():
+    for line in path.read_text().splitlines():
         if line.strip().startswith("traffic_over_algorithmic:"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
@@ -311,7 +323,7 @@ def ours(args, rank, world, local):
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "k_attr_update (attractive CSR pass + gains/momentum update)",
+                         "kernel": f"{ATTR_FORMS[attr_form(d)]}: attractive CSR pass + gains/momentum update",
                          "avg_launch_ms": round(attr_ms, 4), "algorithmic_bytes": attr_bytes,
                          "peak_source": peak_src},
             "e2e": {"value": round(wall_s, 4), "unit": "s", "h2d_bytes_per_step": int(h2d),

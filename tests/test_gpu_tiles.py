@@ -43,6 +43,7 @@ def _wide_tile(P, seed=1):
 
 def _run(P, Y0, iters, tiles, monkeypatch, kind_rows=64):
     monkeypatch.setenv("TSNE_ATTR_TILES", "1" if tiles else "0")
+    monkeypatch.setenv("TSNE_ATTR_PIPE", "0")   # the CSR form the tile form pairs with
     monkeypatch.setenv("TSNE_ATTR_TILES_FROM", "30")
     monkeypatch.setenv("TSNE_ATTR_TILE_ROWS", "32" if kind_rows == 32 else "64")
     eng = Engine(P, Y0, n_iter=200)

@@ -130,12 +130,23 @@ __device__ __forceinline__ void reduce_partials(const double *__restrict__ part,
 // two-kernel form gives the same bits as the fused one.
 enum { ATTR_FUSED = 0, ATTR_GRAD = 1, ATTR_UPDATE = 2 };
 
-template <int D, int MODE, bool CONTIG = false>
-__global__ void __launch_bounds__(ROW_BLOCK)
-k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
-              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
-              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
-              float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
+// The variants with more loads in flight (TSNE_ATTR_PIPE=1 and 2) hold up to 48 registers per
+// thread: five CTAs per SM; form 3 up to 40: six CTAs per SM.
+constexpr int ATTR_PIPE_MINB = 5;
+constexpr int ATTR_PIPE_GRID = 148 * ATTR_PIPE_MINB;
+constexpr int ATTR_PIPE3_MINB = 6;
+constexpr int ATTR_PIPE3_GRID = 148 * ATTR_PIPE3_MINB;
+
+// PF (TSNE_ATTR_PIPE=1): each lane loads its next step's 4 entries of the row before the
+// gathers of the current step; PF = 2 (TSNE_ATTR_PIPE=3): only the next step's 4 columns
+// (the values, which the gathers do not wait for, are loaded with the current step). The same
+// sums in the same order either way.
+template <int D, int MODE, bool CONTIG, int PF>
+__device__ __forceinline__ void
+attr_update_rows(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+                 const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+                 Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+                 float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
 {
     const int lane = threadIdx.x & 31, hl = lane & 15;
     const int half = (blockIdx.x * ROW_BLOCK + threadIdx.x) >> 4;
@@ -196,6 +207,46 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
 #pragma unroll
                 for (int k = 0; k < D; k++) a[k] = vget(s, k);
             }
+        } else if (PF == 2) {
+            int base = b + 4 * hl;
+            int4 c4 = make_int4(0, 0, 0, 0);
+            if (base < e) c4 = ld_stream_i4(col + base);
+            while (base < e) {
+                const int nb = base + 64;
+                const float4 p4 = ld_stream_f4(val + base);
+                int4 cn = c4;
+                if (nb < e) cn = ld_stream_i4(col + nb);
+                attr_acc<D>(yi, Y, c4.x, p4.x, a);
+                attr_acc<D>(yi, Y, c4.y, p4.y, a);
+                attr_acc<D>(yi, Y, c4.z, p4.z, a);
+                attr_acc<D>(yi, Y, c4.w, p4.w, a);
+                c4 = cn;
+                base = nb;
+            }
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+        } else if (PF == 1) {
+            int base = b + 4 * hl;
+            int4 c4 = make_int4(0, 0, 0, 0);
+            float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (base < e) { c4 = ld_stream_i4(col + base); p4 = ld_stream_f4(val + base); }
+            while (base < e) {
+                const int nb = base + 64;
+                int4 cn = c4;
+                float4 pn = p4;
+                if (nb < e) { cn = ld_stream_i4(col + nb); pn = ld_stream_f4(val + nb); }
+                attr_acc<D>(yi, Y, c4.x, p4.x, a);
+                attr_acc<D>(yi, Y, c4.y, p4.y, a);
+                attr_acc<D>(yi, Y, c4.z, p4.z, a);
+                attr_acc<D>(yi, Y, c4.w, p4.w, a);
+                c4 = cn;
+                p4 = pn;
+                base = nb;
+            }
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
         } else {
             for (int base = b + 4 * hl; base < e; base += 64) {
                 const int4 c4 = ld_stream_i4(col + base);
@@ -248,6 +299,193 @@ k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, co
     if (MODE == ATTR_GRAD) return;
     // lanes 0 and 16 of each warp hold partial sums: fold lane 16 into lane 0
     for (int k = 0; k < D; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
+    block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
+}
+
+template <int D, int MODE, bool CONTIG = false>
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_attr_update(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+              float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
+{
+    attr_update_rows<D, MODE, CONTIG, 0>(n, rp, col, val, Y, Yn, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                         partials, attr);
+}
+template <int D, int MODE, bool CONTIG, int PF>
+__global__ void __launch_bounds__(ROW_BLOCK, PF == 1 ? ATTR_PIPE_MINB : ATTR_PIPE3_MINB)
+k_attr_update_pf(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+                 const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+                 Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+                 float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
+{
+    attr_update_rows<D, MODE, CONTIG, PF>(n, rp, col, val, Y, Yn, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                          partials, attr);
+}
+
+// The same step with two rows per half-warp in flight (TSNE_ATTR_PIPE=2): in round rd a
+// half-warp takes rows i0 and i1 = i0 + (half-warps of the split) and loads both rows' next
+// 4 entries per lane before the gathers of either, so every warp keeps four streams of P
+// loads and Y gathers in flight instead of two. Each row's sums run over the same lanes in
+// the same order as in k_attr_update (same bits per row); lane 0 of the half-warp updates i0,
+// lane 1 updates i1 (its operands come from lanes 4-6).
+template <int D, int MODE, bool CONTIG>
+__global__ void __launch_bounds__(ROW_BLOCK, ATTR_PIPE_MINB)
+k_attr_pair(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+            const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+            Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+            float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
+{
+    constexpr int NHC = ROW_BLOCK >> 4;   // half-warps per CTA
+    const int lane = threadIdx.x & 31, hl = lane & 15, hw = (int)threadIdx.x >> 4;
+    const int half = blockIdx.x * NHC + hw;
+    const int nhalf = gridDim.x * NHC;
+    const int use_rep = (MODE != ATTR_GRAD && rep != nullptr) ? *rep_flag : 0;
+    double acc[D];
+    for (int k = 0; k < D; k++) acc[k] = 0.0;
+    __shared__ int s_rng[2];
+    int r0 = 0, r1 = n, rounds;
+    if constexpr (CONTIG) {
+        if (threadIdx.x < 2) {
+            const int c = blockIdx.x + threadIdx.x;
+            int lo = 0;
+            if (c >= (int)gridDim.x) lo = n;
+            else {
+                const long long target = (long long)c * rp[n] / gridDim.x;
+                int hi = n;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (rp[mid] < target) lo = mid + 1;
+                    else hi = mid;
+                }
+            }
+            s_rng[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        r0 = s_rng[0];
+        r1 = s_rng[1];
+        rounds = (r1 - r0 + 2 * NHC - 1) / (2 * NHC);
+    } else {
+        rounds = (n + 2 * nhalf - 1) / (2 * nhalf);
+    }
+    for (int rd = 0; rd < rounds; rd++) {
+        const int i0 = CONTIG ? r0 + rd * 2 * NHC + hw : half + rd * 2 * nhalf;
+        const int i1 = i0 + (CONTIG ? NHC : nhalf);
+        const bool live0 = i0 < r1, live1 = i1 < r1;
+        Vec<D> yi0 = vzero<D>(), yi1 = vzero<D>(), opnd = vzero<D>();
+        int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
+        if (live0) {
+            yi0 = Y[i0];
+            b0 = rp[i0];
+            e0 = rp[i0 + 1];
+            if (MODE != ATTR_GRAD) {
+                if (hl == 1) opnd = uY[i0];
+                else if (hl == 2) opnd = gains[i0];
+                else if (hl == 3 && use_rep) opnd = rep[i0];
+            }
+        }
+        if (live1) {
+            yi1 = Y[i1];
+            b1 = rp[i1];
+            e1 = rp[i1 + 1];
+            if (MODE != ATTR_GRAD) {
+                if (hl == 4) opnd = uY[i1];
+                else if (hl == 5) opnd = gains[i1];
+                else if (hl == 6 && use_rep) opnd = rep[i1];
+            }
+        }
+        float a0[D], a1[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) { a0[k] = 0.f; a1[k] = 0.f; }
+        if (MODE == ATTR_UPDATE) {
+            if (live0 && hl == 0) {
+                const Vec<D> v = attr[i0];
+#pragma unroll
+                for (int k = 0; k < D; k++) a0[k] = vget(v, k);
+            }
+            if (live1 && hl == 1) {
+                const Vec<D> v = attr[i1];
+#pragma unroll
+                for (int k = 0; k < D; k++) a1[k] = vget(v, k);
+            }
+        } else {
+            for (int s0 = b0 + 4 * hl, s1 = b1 + 4 * hl; s0 < e0 || s1 < e1; s0 += 64, s1 += 64) {
+                const bool g0 = s0 < e0, g1 = s1 < e1;
+                int4 c0 = make_int4(0, 0, 0, 0), c1 = make_int4(0, 0, 0, 0);
+                float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (g0) { c0 = ld_stream_i4(col + s0); p0 = ld_stream_f4(val + s0); }
+                if (g1) { c1 = ld_stream_i4(col + s1); p1 = ld_stream_f4(val + s1); }
+                if (g0) {
+                    attr_acc<D>(yi0, Y, c0.x, p0.x, a0);
+                    attr_acc<D>(yi0, Y, c0.y, p0.y, a0);
+                    attr_acc<D>(yi0, Y, c0.z, p0.z, a0);
+                    attr_acc<D>(yi0, Y, c0.w, p0.w, a0);
+                }
+                if (g1) {
+                    attr_acc<D>(yi1, Y, c1.x, p1.x, a1);
+                    attr_acc<D>(yi1, Y, c1.y, p1.y, a1);
+                    attr_acc<D>(yi1, Y, c1.z, p1.z, a1);
+                    attr_acc<D>(yi1, Y, c1.w, p1.w, a1);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                for (int o = 8; o > 0; o >>= 1) {
+                    a0[k] += __shfl_xor_sync(0xffffffffu, a0[k], o);
+                    a1[k] += __shfl_xor_sync(0xffffffffu, a1[k], o);
+                }
+        }
+        if (MODE == ATTR_GRAD) {
+            Vec<D> v = vzero<D>();
+            if (live0 && hl == 0) {
+#pragma unroll
+                for (int k = 0; k < D; k++) vset(v, k, a0[k]);
+                attr[i0] = v;
+            }
+            if (live1 && hl == 1) {
+#pragma unroll
+                for (int k = 0; k < D; k++) vset(v, k, a1[k]);
+                attr[i1] = v;
+            }
+            continue;
+        }
+        // lane 0 of the half updates i0 (operands from lanes 1-3), lane 1 updates i1 (lanes 4-6)
+        const int src = (lane & 16) + (hl == 1 ? 3 : 0);
+        const bool mine = (hl == 0 && live0) || (hl == 1 && live1);
+        Vec<D> u = vzero<D>(), g = vzero<D>(), r = vzero<D>();
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            vset(u, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 1));
+            vset(g, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 2));
+            vset(r, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 3));
+        }
+        if (mine) {
+            const int i = hl == 0 ? i0 : i1;
+            const Vec<D> yi = hl == 0 ? yi0 : yi1;
+            Vec<D> yn = yi;
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                const float gk = exag4 * (hl == 0 ? a0[k] : a1[k]) - vget(r, k);
+                const float uk = vget(u, k);
+                float gain = (uk * gk < 0.f) ? vget(g, k) + 0.2f : vget(g, k) * 0.8f;
+                gain = fmaxf(gain, 0.01f);
+                const float un = mom * uk - lr * (gk * gain);
+                vset(g, k, gain);
+                vset(u, k, un);
+                vset(yn, k, vget(yi, k) + un);
+                acc[k] += (double)vget(yn, k);
+            }
+            uY[i] = u;
+            gains[i] = g;
+            Yn[i] = yn;
+        }
+    }
+    if (MODE == ATTR_GRAD) return;
+    // lanes 0, 1, 16 and 17 of each warp hold partial sums: fold them into lane 0
+    for (int k = 0; k < D; k++) {
+        acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
+        acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 1);
+    }
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
 }
 
@@ -737,11 +975,28 @@ int window_form(int n)
     if (f == 0) return 0;
     return ceil_div(n, f * WIN_GRID) <= win_pts<D>() / f / 2 ? f : 0;
 }
+// Form of the attractive step, TSNE_ATTR_PIPE: 0 k_attr_update (32 registers in 2D, eight CTAs
+// per SM); 1 the same with the next step's entries loaded ahead (48 registers, five CTAs per
+// SM); 2 k_attr_pair (two rows per half-warp, five CTAs per SM); 3 the next step's columns
+// loaded ahead (40 registers, six CTAs per SM). Measured at 1M points, 2D, per launch: 0.619,
+// 0.608, 0.616 and 0.592 ms, so 2D takes form 3 by default. In 3D the fused kernel holds 48
+// registers in every form (five CTAs per SM), and form 3 spills there, so 3D takes form 1,
+// whose grid is one wave of five CTAs per SM. All three modes of a step follow the same form.
+template <int D>
+int attr_pipe()
+{
+    const char *e = getenv("TSNE_ATTR_PIPE");
+    if (e == nullptr || *e == '\0') return D == 2 ? 3 : 1;
+    const int x = atoi(e);
+    return (x >= 1 && x <= 3) ? x : 0;
+}
 template <int D>
 int attr_blocks(int n)
 {
     const int form = window_form<D>(n);
-    return form == 0 ? ROW_GRID : form * WIN_GRID;
+    if (form != 0) return form * WIN_GRID;
+    const int pipe = attr_pipe<D>();
+    return pipe == 3 ? ATTR_PIPE3_GRID : pipe != 0 ? ATTR_PIPE_GRID : ROW_GRID;
 }
 template <int D, int MODE, int FORM>
 void launch_window_form(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
@@ -790,6 +1045,42 @@ int attr_contig()
     return v;
 }
 
+template <int D, int MODE, bool CONTIG>
+void launch_attr_rows(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
+                      void *Ynext, void *uY, void *gains, const void *rep, const int *rep_flag, float exag4,
+                      float mom, float lr, double *partials, void *attr)
+{
+    const int pipe = attr_pipe<D>();
+    if (pipe == 2)
+        k_attr_pair<D, MODE, CONTIG><<<ATTR_PIPE_GRID, ROW_BLOCK, 0, st>>>(
+            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+    else if (pipe == 3)
+        k_attr_update_pf<D, MODE, CONTIG, 2><<<ATTR_PIPE3_GRID, ROW_BLOCK, 0, st>>>(
+            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+    else if (pipe == 1)
+        k_attr_update_pf<D, MODE, CONTIG, 1><<<ATTR_PIPE_GRID, ROW_BLOCK, 0, st>>>(
+            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+    else
+        k_attr_update<D, MODE, CONTIG><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
+            n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+            (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+}
+template <int D, int MODE>
+void launch_attr_any(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
+                     void *Ynext, void *uY, void *gains, const void *rep, const int *rep_flag, float exag4,
+                     float mom, float lr, double *partials, void *attr)
+{
+    if (attr_contig())
+        launch_attr_rows<D, MODE, true>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                        partials, attr);
+    else
+        launch_attr_rows<D, MODE, false>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                         partials, attr);
+}
+
 template <int D>
 void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, const float *val,
                         const void *Y, void *Ynext, void *uY, void *gains, const void *rep,
@@ -800,14 +1091,8 @@ void launch_attr_update(cudaStream_t st, int n, const int *rp, const int *col, c
                                      partials, nullptr);
         return;
     }
-    if (attr_contig())
-        k_attr_update<D, ATTR_FUSED, true><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
-    else
-        k_attr_update<D, ATTR_FUSED><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, nullptr);
+    launch_attr_any<D, ATTR_FUSED>(st, n, rp, col, val, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom, lr,
+                                   partials, nullptr);
 }
 template <int D>
 void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, const float *val, const void *Y,
@@ -818,14 +1103,8 @@ void launch_attr_grad(cudaStream_t st, int n, const int *rp, const int *col, con
                                     0.f, nullptr, attr);
         return;
     }
-    if (attr_contig())
-        k_attr_update<D, ATTR_GRAD, true><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, col, val, (const Vec<D> *)Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, 0.f, nullptr,
-        (Vec<D> *)attr);
-    else
-        k_attr_update<D, ATTR_GRAD><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, col, val, (const Vec<D> *)Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, 0.f, nullptr,
-        (Vec<D> *)attr);
+    launch_attr_any<D, ATTR_GRAD>(st, n, rp, col, val, Y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f,
+                                  0.f, nullptr, attr);
 }
 template <int D>
 void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Ynext, void *uY, void *gains,
@@ -837,14 +1116,8 @@ void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Y
                                       lr, partials, const_cast<void *>(attr));
         return;
     }
-    if (attr_contig())
-        k_attr_update<D, ATTR_UPDATE, true><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, nullptr, nullptr, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
-    else
-        k_attr_update<D, ATTR_UPDATE><<<ROW_GRID, ROW_BLOCK, 0, st>>>(
-        n, rp, nullptr, nullptr, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
-        (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+    launch_attr_any<D, ATTR_UPDATE>(st, n, rp, nullptr, nullptr, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom,
+                                    lr, partials, const_cast<void *>(attr));
 }
 
 template <int D>

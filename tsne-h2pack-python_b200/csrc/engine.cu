@@ -471,7 +471,8 @@ int run_range_impl(tsne_workspace *ws, int it_begin, int it_end)
     }
     // the shared-column tile form of the 2D attractive pass (TSNE_ATTR_TILES=1; off by default
     // until it measures faster), built at the renumberings from iteration tiles_from on
-    const bool tiles_on = env_int("TSNE_ATTR_TILES", 0) != 0 && window_off();
+    const bool tiles_on = env_int("TSNE_ATTR_TILES", 0) != 0 && window_off() && getenv("TSNE_ATTR_PIPE") != nullptr &&
+                          env_int("TSNE_ATTR_PIPE", 0) == 0;
     const int tiles_from = env_int("TSNE_ATTR_TILES_FROM", 100);
     const int tile_rows = env_int("TSNE_ATTR_TILE_ROWS", 64), tile_umax = env_int("TSNE_ATTR_TILE_UMAX", 6144);
     const int h2_freq = p.h2_rebuild_freq > 0 ? p.h2_rebuild_freq : 10;

@@ -57,7 +57,7 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 # traffic per algorithmic byte scales the traffic to this workload's launch
 TRAFFIC = [ROOT / "profiles" / "k_attr_update_pf_200k_full.md", ROOT / "profiles" / "k_attr_update_200k_full.md"]
 
-# the attractive step's form (TSNE_ATTR_PIPE; default 3 in 2D, 1 in 3D), as the engine picks it
+# the attractive step's form (TSNE_ATTR_PIPE; default 3 in 2D, 0 in 3D), as the engine picks it
 ATTR_FORMS = {0: "k_attr_update", 1: "k_attr_update_pf<1> (next step's entries loaded ahead)",
               2: "k_attr_pair (two rows per half-warp)", 3: "k_attr_update_pf<2> (next step's columns loaded ahead)"}
 
@@ -65,7 +65,7 @@ ATTR_FORMS = {0: "k_attr_update", 1: "k_attr_update_pf<1> (next step's entries l
 def attr_form(d):
     v = os.environ.get("TSNE_ATTR_PIPE", "")
     if v == "":
-        return 3 if d == 2 else 1
+        return 3 if d == 2 else 0
     return int(v) if v.isdigit() and int(v) in ATTR_FORMS else 0
 
 

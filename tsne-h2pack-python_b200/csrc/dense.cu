@@ -323,6 +323,48 @@ k_attr_update_pf(int n, const int *__restrict__ rp, const int *__restrict__ col,
                                           partials, attr);
 }
 
+// The update of a rebuild iteration from its stored attractive sums, for the forms with more
+// loads in flight (TSNE_ATTR_PIPE 1-3): a thread per row, rows strided over the form's grid (so
+// the centring reads as many partials as after a fused step), each row's arithmetic that of
+// the fused step. The half-warp-per-row update of form 0 keeps 16 lanes per row for three
+// loads; this one reads and writes every array coalesced.
+template <int D>
+__global__ void __launch_bounds__(ROW_BLOCK)
+k_update_rows(int n, const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+              const Vec<D> *__restrict__ attr, float exag4, float mom, float lr, double *__restrict__ partials)
+{
+    const int use_rep = rep != nullptr ? *rep_flag : 0;
+    double acc[D];
+#pragma unroll
+    for (int k = 0; k < D; k++) acc[k] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> yi = Y[i], sa = attr[i];
+        Vec<D> u = uY[i], g = gains[i];
+        const Vec<D> r = use_rep ? rep[i] : vzero<D>();
+        Vec<D> yn = yi;
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            const float gk = exag4 * vget(sa, k) - vget(r, k);
+            const float uk = vget(u, k);
+            float gain = (uk * gk < 0.f) ? vget(g, k) + 0.2f : vget(g, k) * 0.8f;
+            gain = fmaxf(gain, 0.01f);
+            const float un = mom * uk - lr * (gk * gain);
+            vset(g, k, gain);
+            vset(u, k, un);
+            vset(yn, k, vget(yi, k) + un);
+            acc[k] += (double)vget(yn, k);
+        }
+        uY[i] = u;
+        gains[i] = g;
+        Yn[i] = yn;
+    }
+#pragma unroll
+    for (int k = 0; k < D; k++)
+        for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+    block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
+}
+
 // The same step with two rows per half-warp in flight (TSNE_ATTR_PIPE=2): in round rd a
 // half-warp takes rows i0 and i1 = i0 + (half-warps of the split) and loads both rows' next
 // 4 entries per lane before the gathers of either, so every warp keeps four streams of P
@@ -980,13 +1022,14 @@ int window_form(int n)
 // SM); 2 k_attr_pair (two rows per half-warp, five CTAs per SM); 3 the next step's columns
 // loaded ahead (40 registers, six CTAs per SM). Measured at 1M points, 2D, per launch: 0.619,
 // 0.608, 0.616 and 0.592 ms, so 2D takes form 3 by default. In 3D the fused kernel holds 48
-// registers in every form (five CTAs per SM), and form 3 spills there, so 3D takes form 1,
-// whose grid is one wave of five CTAs per SM. All three modes of a step follow the same form.
+// registers in every form and form 3 spills there; form 1 measured no faster than form 0 at
+// 500K points (0.352 against 0.348 ms per launch), so 3D keeps form 0. The attractive sums of a
+// rebuild iteration follow the form; their update is k_update_rows for forms 1-3.
 template <int D>
 int attr_pipe()
 {
     const char *e = getenv("TSNE_ATTR_PIPE");
-    if (e == nullptr || *e == '\0') return D == 2 ? 3 : 1;
+    if (e == nullptr || *e == '\0') return D == 2 ? 3 : 0;
     const int x = atoi(e);
     return (x >= 1 && x <= 3) ? x : 0;
 }
@@ -1114,6 +1157,12 @@ void launch_update(cudaStream_t st, int n, const int *rp, const void *Y, void *Y
     if (window_form<D>(n) != 0) {
         launch_window<D, ATTR_UPDATE>(st, n, rp, nullptr, nullptr, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom,
                                       lr, partials, const_cast<void *>(attr));
+        return;
+    }
+    if (attr_pipe<D>() != 0) {
+        k_update_rows<D><<<attr_blocks<D>(n), ROW_BLOCK, 0, st>>>(
+            n, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains, (const Vec<D> *)rep, rep_flag,
+            (const Vec<D> *)attr, exag4, mom, lr, partials);
         return;
     }
     launch_attr_any<D, ATTR_UPDATE>(st, n, rp, nullptr, nullptr, Y, Ynext, uY, gains, rep, rep_flag, exag4, mom,

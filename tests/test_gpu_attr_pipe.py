@@ -2,7 +2,8 @@
 
   - 1: each lane loads its next 4 entries of the row before the current gathers;
   - 2: two rows per half-warp (k_attr_pair);
-  - 3: each lane loads its next 4 columns before the current gathers.
+  - 3: each lane loads its next 4 columns before the current gathers;
+  - 4: the same across the rows of a half-warp (k_attr_stream).
 
 Both keep every row's sums over the same lanes in the same order, so a run equals the default
 run through iteration 32 (past the renumbering at 30) to rel 1e-6 (only the centring mean's
@@ -35,7 +36,7 @@ def _run(P, Y0, iters, pipe, monkeypatch):
 
 
 @pytest.mark.parametrize("kind", ["plain", "ragged"])
-@pytest.mark.parametrize("pipe", [1, 2, 3])
+@pytest.mark.parametrize("pipe", [1, 2, 3, 4])
 def test_pipe_forms_equal_default(mid, kind, pipe, monkeypatch):
     X, G, P, _ = mid
     if kind == "ragged":

@@ -365,6 +365,150 @@ k_update_rows(int n, const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<
     block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
 }
 
+// The step as one stream of 64-entry steps per half-warp (TSNE_ATTR_PIPE=4): the next step's
+// columns are loaded before the current gathers across row boundaries too: during a row's last
+// step the lanes load the first columns of the half-warp's next row, whose row pointers and Y
+// are loaded when the current row starts. So a row of more than one step waits on no
+// row-pointer or column load, only on its gathers. Each row's sums run over the same
+// lanes in the same order as in k_attr_update (same bits per row); a rebuild iteration's
+// update is k_update_rows.
+template <int D, int MODE, bool CONTIG>
+__global__ void __launch_bounds__(ROW_BLOCK, ATTR_PIPE_MINB)
+k_attr_stream(int n, const int *__restrict__ rp, const int *__restrict__ col, const float *__restrict__ val,
+              const Vec<D> *__restrict__ Y, Vec<D> *__restrict__ Yn, Vec<D> *__restrict__ uY,
+              Vec<D> *__restrict__ gains, const Vec<D> *__restrict__ rep, const int *__restrict__ rep_flag,
+              float exag4, float mom, float lr, double *__restrict__ partials, Vec<D> *__restrict__ attr)
+{
+    static_assert(MODE != ATTR_UPDATE, "the update of a rebuild iteration is k_update_rows");
+    constexpr int NHC = ROW_BLOCK >> 4;   // half-warps per CTA
+    const int lane = threadIdx.x & 31, hl = lane & 15, hw = (int)threadIdx.x >> 4;
+    const int half = blockIdx.x * NHC + hw;
+    const int nhalf = gridDim.x * NHC;
+    const int use_rep = (MODE != ATTR_GRAD && rep != nullptr) ? *rep_flag : 0;
+    double acc[D];
+    for (int k = 0; k < D; k++) acc[k] = 0.0;
+    __shared__ int s_rng[2];
+    int r0 = 0, r1 = n, rounds, first, stride;
+    if constexpr (CONTIG) {
+        if (threadIdx.x < 2) {
+            const int c = blockIdx.x + threadIdx.x;
+            int lo = 0;
+            if (c >= (int)gridDim.x) lo = n;
+            else {
+                const long long target = (long long)c * rp[n] / gridDim.x;
+                int hi = n;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (rp[mid] < target) lo = mid + 1;
+                    else hi = mid;
+                }
+            }
+            s_rng[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        r0 = s_rng[0];
+        r1 = s_rng[1];
+        rounds = (r1 - r0 + NHC - 1) / NHC;
+        first = r0 + hw;
+        stride = NHC;
+    } else {
+        rounds = (n + nhalf - 1) / nhalf;
+        first = half;
+        stride = nhalf;
+    }
+    // the current row (i) and the next (i + stride)
+    int i = first;
+    bool live = i < r1;
+    Vec<D> yi = vzero<D>();
+    int b = 0, e = 0;
+    if (live) { yi = Y[i]; b = rp[i]; e = rp[i + 1]; }
+    int4 c4 = make_int4(0, 0, 0, 0);
+    if (b + 4 * hl < e) c4 = ld_stream_i4(col + b + 4 * hl);
+    for (int rd = 0; rd < rounds; rd++) {
+        const int i_n = i + stride;
+        const bool live_n = i_n < r1;
+        Vec<D> yi_n = vzero<D>(), opnd = vzero<D>();
+        int nb = 0, ne = 0;
+        if (live_n) { yi_n = Y[i_n]; nb = rp[i_n]; ne = rp[i_n + 1]; }
+        if (MODE != ATTR_GRAD && live) {
+            if (hl == 1) opnd = uY[i];
+            else if (hl == 2) opnd = gains[i];
+            else if (hl == 3 && use_rep) opnd = rep[i];
+        }
+        float a[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) a[k] = 0.f;
+        const int nch = (e - b + 63) >> 6;   // steps of this row, the same for the half-warp
+        int base = b + 4 * hl;
+        for (int s = 0; s < nch; s++) {
+            float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (base < e) p4 = ld_stream_f4(val + base);
+            const bool last = s + 1 == nch;
+            const int na = last ? nb + 4 * hl : base + 64, nae = last ? ne : e;
+            int4 cn = make_int4(0, 0, 0, 0);
+            if (na < nae) cn = ld_stream_i4(col + na);
+            if (base < e) {
+                attr_acc<D>(yi, Y, c4.x, p4.x, a);
+                attr_acc<D>(yi, Y, c4.y, p4.y, a);
+                attr_acc<D>(yi, Y, c4.z, p4.z, a);
+                attr_acc<D>(yi, Y, c4.w, p4.w, a);
+            }
+            c4 = cn;
+            base += 64;
+        }
+        if (nch == 0) {   // an empty (or absent) row: the next row's first columns now
+            c4 = make_int4(0, 0, 0, 0);
+            if (nb + 4 * hl < ne) c4 = ld_stream_i4(col + nb + 4 * hl);
+        }
+#pragma unroll
+        for (int k = 0; k < D; k++)
+            for (int o = 8; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+        if (MODE == ATTR_GRAD) {
+            if (live && hl == 0) {
+                Vec<D> v = vzero<D>();
+#pragma unroll
+                for (int k = 0; k < D; k++) vset(v, k, a[k]);
+                attr[i] = v;
+            }
+        } else {
+            const int src = lane & 16;
+            Vec<D> u = vzero<D>(), g = vzero<D>(), r = vzero<D>();
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                vset(u, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 1));
+                vset(g, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 2));
+                vset(r, k, __shfl_sync(0xffffffffu, vget(opnd, k), src + 3));
+            }
+            if (live && hl == 0) {
+                Vec<D> yn = yi;
+#pragma unroll
+                for (int k = 0; k < D; k++) {
+                    const float gk = exag4 * a[k] - vget(r, k);
+                    const float uk = vget(u, k);
+                    float gain = (uk * gk < 0.f) ? vget(g, k) + 0.2f : vget(g, k) * 0.8f;
+                    gain = fmaxf(gain, 0.01f);
+                    const float un = mom * uk - lr * (gk * gain);
+                    vset(g, k, gain);
+                    vset(u, k, un);
+                    vset(yn, k, vget(yi, k) + un);
+                    acc[k] += (double)vget(yn, k);
+                }
+                uY[i] = u;
+                gains[i] = g;
+                Yn[i] = yn;
+            }
+        }
+        i = i_n;
+        live = live_n;
+        yi = yi_n;
+        b = nb;
+        e = ne;
+    }
+    if (MODE == ATTR_GRAD) return;
+    for (int k = 0; k < D; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
+    block_sum_warps<D>(acc, partials + (size_t)blockIdx.x * D);
+}
+
 // The same step with two rows per half-warp in flight (TSNE_ATTR_PIPE=2): in round rd a
 // half-warp takes rows i0 and i1 = i0 + (half-warps of the split) and loads both rows' next
 // 4 entries per lane before the gathers of either, so every warp keeps four streams of P
@@ -1020,8 +1164,9 @@ int window_form(int n)
 // Form of the attractive step, TSNE_ATTR_PIPE: 0 k_attr_update (32 registers in 2D, eight CTAs
 // per SM); 1 the same with the next step's entries loaded ahead (48 registers, five CTAs per
 // SM); 2 k_attr_pair (two rows per half-warp, five CTAs per SM); 3 the next step's columns
-// loaded ahead (40 registers, six CTAs per SM). Measured at 1M points, 2D, per launch: 0.619,
-// 0.608, 0.616 and 0.592 ms, so 2D takes form 3 by default. In 3D the fused kernel holds 48
+// loaded ahead (40 registers, six CTAs per SM); 4 k_attr_stream (the column loads ahead across
+// the rows of a half-warp, five CTAs per SM). Measured at 1M points, 2D, per launch: 0.619,
+// 0.608, 0.616, 0.592 and 0.634 ms, so 2D takes form 3 by default. In 3D the fused kernel holds 48
 // registers in every form and form 3 spills there; form 1 measured no faster than form 0 at
 // 500K points (0.352 against 0.348 ms per launch), so 3D keeps form 0. The attractive sums of a
 // rebuild iteration follow the form; their update is k_update_rows for forms 1-3.
@@ -1031,7 +1176,7 @@ int attr_pipe()
     const char *e = getenv("TSNE_ATTR_PIPE");
     if (e == nullptr || *e == '\0') return D == 2 ? 3 : 0;
     const int x = atoi(e);
-    return (x >= 1 && x <= 3) ? x : 0;
+    return (x >= 1 && x <= 4) ? x : 0;
 }
 template <int D>
 int attr_blocks(int n)
@@ -1094,6 +1239,14 @@ void launch_attr_rows(cudaStream_t st, int n, const int *rp, const int *col, con
                       float mom, float lr, double *partials, void *attr)
 {
     const int pipe = attr_pipe<D>();
+    if constexpr (MODE != ATTR_UPDATE) {
+        if (pipe == 4) {
+            k_attr_stream<D, MODE, CONTIG><<<ATTR_PIPE_GRID, ROW_BLOCK, 0, st>>>(
+                n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,
+                (const Vec<D> *)rep, rep_flag, exag4, mom, lr, partials, (Vec<D> *)attr);
+            return;
+        }
+    }
     if (pipe == 2)
         k_attr_pair<D, MODE, CONTIG><<<ATTR_PIPE_GRID, ROW_BLOCK, 0, st>>>(
             n, rp, col, val, (const Vec<D> *)Y, (Vec<D> *)Ynext, (Vec<D> *)uY, (Vec<D> *)gains,

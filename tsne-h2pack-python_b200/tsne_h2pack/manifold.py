@@ -219,6 +219,7 @@ class TSNE:
         """Embed X (features, or a sparse k-NN distance graph with metric='precomputed')."""
         if self.metric == "precomputed":
             return self._fit_transform_precomputed(X)
+        X_in = X
         X = self._validate_data(X)
         init_Y = self._initial_embedding(X, X.shape[0])
         backend = get_backend()
@@ -233,7 +234,10 @@ class TSNE:
         k = min(X.shape[0] - 1, int(3 * self.perplexity))
         if self.verbose:
             print(f"Computing {k} nearest neighbors using {self.knn_method}...")
-        G = knn.compute(X, k=k, n_jobs=self.n_jobs, verbose=(self.verbose > 0), **self.knn_params)
+        # the device k-NN reads single precision: it takes the caller's float32 array when there
+        # is one (the float64 copy rounds back to the same values) instead of converting again
+        Xk = X_in if (self.knn_method == "cuda" and isinstance(X_in, np.ndarray) and X_in.dtype == np.float32) else X
+        G = knn.compute(Xk, k=k, n_jobs=self.n_jobs, verbose=(self.verbose > 0), **self.knn_params)
         self.knn_time_ = getattr(G, "knn_time", 0.0)
         Y, metrics = backend.fit_transform_with_knn_distances(X, G, self.n_components, params, init_Y=init_Y)
         self.embedding_ = Y

@@ -90,3 +90,15 @@ def test_tensor_core_scan_against_cuda_core_scan(n, dim, k, monkeypatch):
     assert ok_tc >= ok_fp - 1e-3
     if dim > 64:
         assert same == 1.0
+
+
+def test_fit_transform_float32_input_equals_float64_copy():
+    """TSNE(knn_method='cuda') hands a float32 X straight to the device k-NN; the float64 copy of
+    the same values gives the same graph and the same embedding, bit for bit."""
+    from tsne_h2pack import TSNE
+    rng = np.random.default_rng(11)
+    X = (rng.standard_normal((3000, 20)) + np.repeat(rng.normal(0, 4, (6, 20)), 500, axis=0)).astype(np.float32)
+    kw = dict(n_components=2, perplexity=30, max_iter=60, init="random", random_state=3, knn_method="cuda")
+    Ya = TSNE(**kw).fit_transform(X)
+    Yb = TSNE(**kw).fit_transform(X.astype(np.float64))
+    np.testing.assert_array_equal(Ya, Yb)

@@ -108,3 +108,42 @@ def test_prepare_knn_graph_drops_self_entries_and_sorts():
     np.fill_diagonal(d3, 0.0)
     np.testing.assert_array_equal(out3.toarray(), d3)
     assert not np.any(out3.indices == np.repeat(np.arange(n), np.diff(out3.indptr)))
+
+
+def test_feature_path_hands_float32_to_the_device_knn(monkeypatch):
+    """knn_method='cuda' gets the caller's float32 array itself (validated, not copied); the
+    other methods get the float64 copy the reference makes; NaN is refused either way. The
+    k-NN and the backend are stand-ins here, so no device is needed."""
+    from scipy.sparse import csr_matrix
+    import tsne_h2pack.manifold as M
+    import tsne_h2pack._knn_methods as K
+    real = M.get_backend()
+    seen = {}
+
+    class FakeKNN:
+        def compute(self, X, k, **kw):
+            seen["knn_X"] = X
+            n = X.shape[0]
+            idx = (np.arange(n)[:, None] + np.arange(1, k + 1)[None, :]) % n
+            return csr_matrix((np.ones(n * k), idx.ravel(), np.arange(0, (n + 1) * k, k)), shape=(n, n))
+
+    class FakeBackend:
+        backend_type = "stand-in"
+        create_default_params = staticmethod(real.create_default_params)
+
+        def fit_transform_with_knn_distances(self, X, G, c, params, init_Y=None):
+            seen["X"] = X
+            return np.zeros((X.shape[0], c)), {"kl_divergence": 0.0, "n_iter": 1}
+
+    monkeypatch.setattr(K, "get_knn_method", lambda name: FakeKNN())
+    monkeypatch.setattr(M, "get_backend", lambda: FakeBackend())
+    X = np.random.default_rng(0).standard_normal((100, 5)).astype(np.float32)
+    TSNE(knn_method="cuda", perplexity=5, init="random").fit_transform(X)
+    assert seen["knn_X"] is X and seen["X"] is X
+    TSNE(knn_method="exact", perplexity=5, init="random").fit_transform(X)
+    assert seen["knn_X"].dtype == np.float64
+    np.testing.assert_array_equal(seen["knn_X"], X.astype(np.float64))
+    Xn = X.copy()
+    Xn[3, 1] = np.nan
+    with pytest.raises(ValueError):
+        TSNE(knn_method="cuda", perplexity=5, init="random").fit_transform(Xn)

@@ -219,8 +219,11 @@ class TSNE:
         """Embed X (features, or a sparse k-NN distance graph with metric='precomputed')."""
         if self.metric == "precomputed":
             return self._fit_transform_precomputed(X)
-        X_in = X
-        X = self._validate_data(X)
+        # the device k-NN reads single precision: a float32 X stays float32 (the float64 copy the
+        # other k-NN methods read would round back to the same values), which saves a conversion
+        # of the whole matrix each way; PCA initialisation converts on its own
+        keep32 = self.knn_method == "cuda" and isinstance(X, np.ndarray) and X.dtype == np.float32
+        X = self._validate_data(X, dtype=np.float32 if keep32 else NP_DTYPE)
         init_Y = self._initial_embedding(X, X.shape[0])
         backend = get_backend()
         params = self._map_params_to_c_struct(n_samples=X.shape[0])
@@ -234,10 +237,7 @@ class TSNE:
         k = min(X.shape[0] - 1, int(3 * self.perplexity))
         if self.verbose:
             print(f"Computing {k} nearest neighbors using {self.knn_method}...")
-        # the device k-NN reads single precision: it takes the caller's float32 array when there
-        # is one (the float64 copy rounds back to the same values) instead of converting again
-        Xk = X_in if (self.knn_method == "cuda" and isinstance(X_in, np.ndarray) and X_in.dtype == np.float32) else X
-        G = knn.compute(Xk, k=k, n_jobs=self.n_jobs, verbose=(self.verbose > 0), **self.knn_params)
+        G = knn.compute(X, k=k, n_jobs=self.n_jobs, verbose=(self.verbose > 0), **self.knn_params)
         self.knn_time_ = getattr(G, "knn_time", 0.0)
         Y, metrics = backend.fit_transform_with_knn_distances(X, G, self.n_components, params, init_Y=init_Y)
         self.embedding_ = Y
@@ -245,8 +245,8 @@ class TSNE:
         self.kl_divergence_ = metrics.get("kl_divergence", 0.0)
         return self.embedding_
 
-    def _validate_data(self, X) -> np.ndarray:
-        X = np.asarray(X, dtype=NP_DTYPE)
+    def _validate_data(self, X, dtype=NP_DTYPE) -> np.ndarray:
+        X = np.asarray(X, dtype=dtype)
         if X.ndim != 2:
             raise ValueError(f"X must be 2-dimensional array, got {X.ndim} dimensions")
         n_samples = X.shape[0]
